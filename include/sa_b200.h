@@ -1,0 +1,128 @@
+/*
+ * sa_b200.h -- C ABI of the B200 multispin-coded Ising spin-glass engine.
+ *
+ * One "system" is one lattice carrying 64 replicas, one bit each, in a 64-bit
+ * word per site: the reference's gpu_sys / cpu_sys object
+ * (src/gpu_sys.cuh:12-29, src/cpu_sys.hpp:12-31). Every entry point:
+ *   - is extern "C", takes plain pointers and sizes, and never throws;
+ *   - returns an int status (SA_OK == 0); sa_last_error() gives a message for
+ *     the calling thread;
+ *   - is safe to call concurrently on DISTINCT handles.
+ * Host buffers use the reference's row-major layout (site i = x + L*y + L*L*z)
+ * and its duplicated coupling layout J?[2N] (J?[2i] = bond to the -x/-y/-z
+ * neighbour, J?[2i+1] = bond to the +x/+y/+z neighbour). Energies cross the
+ * ABI as exact integers per replica bit j (index j = bit j, which is also the
+ * index the reference's float vectors use).
+ *
+ * Random numbers follow the reference GPU schedule (src/random.cu:15-35,
+ * src/device_2d.cu:96-97): site i draws from Philox4x32-10 stream
+ * (key = seed, subsequence = i); every site consumes one draw per half-sweep,
+ * so a system's whole RNG state is (seed, draw counter).
+ */
+#ifndef SA_B200_H
+#define SA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------- */
+enum {
+  SA_OK = 0,
+  SA_ERR_INVALID = 1,      /* bad argument (null pointer, size, range) */
+  SA_ERR_ODD_L = 2,        /* L must be even (checkerboard colouring) */
+  SA_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+  SA_ERR_NO_DEVICE = 4,    /* no CUDA device / extension unusable */
+  SA_ERR_MISMATCH = 5,     /* two systems of different shape */
+  SA_ERR_J_INCONSISTENT = 6, /* duplicated coupling words disagree */
+  SA_ERR_BUFFER = 7,       /* caller buffer too small / bad checkpoint */
+  SA_ERR_BUDGET = 8,       /* memory budget exceeded */
+  SA_ERR_TIMEOUT = 9,      /* a bounded device-side wait gave up */
+  SA_ERR_UNSUPPORTED = 10  /* valid request this build does not handle */
+};
+
+/* lattice kinds (the reference classes they replace) */
+enum {
+  SA_LATTICE_2D = 0,        /* cpu_2d: square, periodic in x and y */
+  SA_LATTICE_2D_OPEN_X = 1, /* cpu_2dp / gpu_2d: open in x, periodic in y */
+  SA_LATTICE_3D = 2         /* cpu_3d / gpu_3d: cubic, periodic */
+};
+
+typedef struct sa_system* sa_system_t;
+
+/* Last error message of the calling thread ("" if none). */
+const char* sa_last_error(void);
+/* Static description of a status code. */
+const char* sa_status_string(int status);
+/* Library version string. */
+const char* sa_version(void);
+
+/* ---- single systems: the gpu_sys boundary ----------------------------------- */
+
+/* Constructor: gpu_2d(L,T,h) src/gpu_2d.cu:23-84, gpu_3d(L,T,h) src/gpu_3d.cu:20-77.
+ * Allocates spins and couplings on the current device, keys the generator with
+ * seed 1234 (src/gpu_2d.cu:47) and zeroes spins and couplings. */
+int sa_sys_create(int lattice, int L, double T, double h, sa_system_t* out);
+/* gpu_free() + delete: src/gpu_2d.cu:90-107. */
+int sa_sys_destroy(sa_system_t sys);
+/* Run this system's work on `stream` (a cudaStream_t; NULL = the system's own). */
+int sa_sys_set_stream(sa_system_t sys, void* stream);
+/* set_T: src/gpu_2d.cu:122-147 (Boltzmann table -> integer thresholds). */
+int sa_sys_set_T(sa_system_t sys, double T);
+/* set_h: src/gpu_2d.cu:149-173. */
+int sa_sys_set_h(sa_system_t sys, double h);
+int sa_sys_get_T(sa_system_t sys, double* T);
+/* set_seed: src/gpu_3d.cu:205-210 (re-keys every site's stream, draw counter 0). */
+int sa_sys_set_seed(sa_system_t sys, uint64_t seed);
+/* init_J: src/gpu_2d.cu:247-257 (2*dim draws per site -> own bond words). */
+int sa_sys_init_J(sa_system_t sys);
+/* init_rand: src/gpu_2d.cu:259-264. Counter-based here: site i takes Philox
+ * block (epoch, 0, i, 2^31 | i>>32) of key seed; each call advances the epoch. */
+int sa_sys_init_rand(sa_system_t sys);
+/* init_order: src/cpu_2dp.cpp:296-301 (all spins up). */
+int sa_sys_init_order(sa_system_t sys);
+/* load_J / save_J data path (src/gpu_2d.cu:213-244): host arrays of 2N words
+ * each, jz ignored for 2D. set_J rejects duplicated words that disagree. */
+int sa_sys_set_J(sa_system_t sys, const uint64_t* jx, const uint64_t* jy, const uint64_t* jz);
+int sa_sys_get_J(sa_system_t sys, uint64_t* jx, uint64_t* jy, uint64_t* jz);
+/* Spins, host row-major, N words. */
+int sa_sys_set_spins(sa_system_t sys, const uint64_t* s);
+int sa_sys_get_spins(sa_system_t sys, uint64_t* s);
+/* sweep(): src/gpu_2d.cu:109-120 -- here `nsweeps` full sweeps, two
+ * half-sweep launches each, asynchronous on the system's stream. */
+int sa_sys_sweep(sa_system_t sys, long nsweeps);
+/* measure(): src/gpu_2d.cu:176-211. E[j] = sum over bonds of (+1 satisfied,
+ * -1 not), M[j] = sum over sites of (+1 up, -1 down), j = replica bit. Host
+ * outputs; synchronises the system's stream. */
+int sa_sys_measure(sa_system_t sys, int64_t* E, int64_t* M);
+/* The reference's float vector: out[j] = (float)(E[j] + h*M[j]). */
+int sa_sys_measure_float(sa_system_t sys, float* out64);
+/* Device-side measure into DEVICE arrays E[64], M[64] (int64), asynchronous. */
+int sa_sys_measure_async(sa_system_t sys, int64_t* d_E, int64_t* d_M);
+/* swap(sys, mask): src/gpu_2d.cu:305-324 -- bit-masked exchange of all spin
+ * words between two systems of the same shape (src/tools_inline.hpp:4-9). */
+int sa_sys_swap(sa_system_t a, sa_system_t b, uint64_t mask);
+/* get_N: src/gpu_2d.cu:301-303. */
+int sa_sys_get_N(sa_system_t sys, long* N);
+/* RNG position (for checkpoints): draw counter and spin-init epoch. */
+int sa_sys_get_rng(sa_system_t sys, uint64_t* seed, uint64_t* draw, uint64_t* epoch);
+int sa_sys_set_rng(sa_system_t sys, uint64_t seed, uint64_t draw, uint64_t epoch);
+/* Wait for the system's queued work. */
+int sa_sys_sync(sa_system_t sys);
+/* save()/load() replacement (src/gpu_2d.cu:327-412): a self-describing
+ * checkpoint (lattice, L, T, h, seed, draw, epoch, spins, own couplings).
+ * sa_sys_save with buf==NULL reports the size in *len. */
+int sa_sys_save(sa_system_t sys, void* buf, size_t cap, size_t* len);
+int sa_sys_load(sa_system_t sys, const void* buf, size_t len);
+
+/* Device pointers of the internal layout (read-only use by advanced callers):
+ * spins [colour][row][k] and own couplings [axis][colour][row][k]. */
+int sa_sys_device_buffers(sa_system_t sys, uint64_t** d_spins, uint64_t** d_J);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SA_B200_H */

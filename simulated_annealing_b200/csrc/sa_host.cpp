@@ -1,0 +1,130 @@
+// sa_host.cpp -- host helpers: error state, Boltzmann tables, thresholds and
+// the exchange-decision intervals. Compiled with -ffp-contract=off so every
+// expression rounds exactly like the reference's host code.
+#include "sa_host.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "sa_b200.h"
+
+namespace sa {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int status, const std::string& msg) {
+  g_last_error = msg;
+  return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  char buf[512];
+  snprintf(buf, sizeof buf, "CUDA error %d (%s) in %s", (int)e, cudaGetErrorString(e), what);
+  g_last_error = buf;
+  return SA_ERR_CUDA;
+}
+
+void boltz_table(int lattice, double T, double h, double* b) {
+  for (int i = 0; i < 20; ++i) b[i] = 0.0;
+  if (lattice == SA_LATTICE_3D) {
+    for (size_t i = 0; i < 7; i++) {
+      int j = ((int)i - 3) * 2;
+      b[i] = std::min(1., exp(-2 * (1 / T) * (j - h)));
+      b[7 + i] = std::min(1., exp(-2 * (1 / T) * (j + h)));
+    }
+  } else {
+    for (size_t i = 0; i < 5; i++) {
+      int j = ((int)i - 2) * 2;
+      b[i] = std::min(1., exp(-2 * (1 / T) * (j - h)));
+      b[5 + i] = std::min(1., exp(-2 * (1 / T) * (j + h)));
+      b[10 + i] = std::min(1., (i == 0) ? 0. : exp(-2 * (1 / T) * (j - 1 - h)));
+      b[15 + i] = std::min(1., (i == 0) ? 0. : exp(-2 * (1 / T) * (j - 1 + h)));
+    }
+  }
+}
+
+float uniform_from_u32(uint32_t u) {
+  volatile float fu = (float)u;
+  volatile float scaled = fu * 0x1p-32f;
+  return scaled + 0x1p-33f;
+}
+
+uint32_t threshold_of(float b) {
+  uint64_t lo = 0, hi = 1ULL << 32;
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (uniform_from_u32((uint32_t)mid) < b) lo = mid + 1; else hi = mid;
+  }
+  // b <= 1.0 always (min(1, .)), and uniform(2^32-1) == 1.0, so lo < 2^32.
+  return lo >= (1ULL << 32) ? 0xFFFFFFFFu : (uint32_t)lo;
+}
+
+bool make_thresholds(int lattice, double T, double h, Thresholds* t) {
+  double b[20];
+  boltz_table(lattice, T, h, b);
+  memset(t, 0, sizeof *t);
+  int nb = (lattice == SA_LATTICE_3D) ? 6 : 4;
+  int up0 = nb + 1;
+  for (int k = 0; k <= nb; ++k) {
+    t->dn[k] = threshold_of((float)b[k]);
+    t->up[k] = threshold_of((float)b[up0 + k]);
+  }
+  if (lattice != SA_LATTICE_3D) {
+    for (int k = 0; k <= 4; ++k) {
+      t->bdn[k] = threshold_of((float)b[10 + k]);
+      t->bup[k] = threshold_of((float)b[15 + k]);
+    }
+    // A border site always has its forced bond satisfied, so k >= 1 and the
+    // k = 0 entry (0 in the reference) is never consulted; copying k = 1
+    // keeps the prefix property the kernels rely on.
+    t->bdn[0] = t->bdn[1];
+    t->bup[0] = t->bup[1];
+  }
+  for (int k = 1; k <= nb; ++k)
+    if (t->dn[k] > t->dn[k - 1] || t->up[k] > t->up[k - 1]) return false;
+  if (lattice != SA_LATTICE_3D)
+    for (int k = 1; k <= 4; ++k)
+      if (t->bdn[k] > t->bdn[k - 1] || t->bup[k] > t->bup[k - 1]) return false;
+  return true;
+}
+
+bool pt_accept(float dE, double dB, double r) {
+  return ((dE * dB) > 0.) || r < exp(dB * dE);
+}
+
+void pt_accept_interval(double dB, double r, int64_t span, int64_t* lo, int64_t* hi) {
+  auto acc = [&](int64_t x) { return pt_accept((float)x, dB, r); };
+  if (!(dB > 0) && !(dB < 0)) {  // dB == 0: exp(0) = 1 > r, every dE accepted
+    *lo = -span;
+    *hi = span;
+    return;
+  }
+  if (dB > 0) {
+    // accepted set is [D, span]; acc(0) holds because r < 1 = exp(0).
+    int64_t a = -span, b = 0;  // smallest accepted in [a, b]
+    if (acc(a)) { *lo = a; *hi = span; return; }
+    while (b - a > 1) {
+      int64_t m = a + (b - a) / 2;
+      if (acc(m)) b = m; else a = m;
+    }
+    *lo = b;
+    *hi = span;
+  } else {
+    int64_t a = 0, b = span;  // largest accepted in [a, b]
+    if (acc(b)) { *lo = -span; *hi = b; return; }
+    while (b - a > 1) {
+      int64_t m = a + (b - a) / 2;
+      if (acc(m)) a = m; else b = m;
+    }
+    *lo = -span;
+    *hi = a;
+  }
+}
+
+}  // namespace sa
+
+extern "C" const char* sa_last_error(void) { return sa::g_last_error.c_str(); }

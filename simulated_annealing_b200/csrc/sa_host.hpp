@@ -1,0 +1,48 @@
+// sa_host.hpp -- host-side helpers shared by the engine's translation units:
+// error state, Boltzmann tables, integer thresholds, PT decision intervals.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "sa_device.cuh"
+
+namespace sa {
+
+// Per-thread last-error message behind sa_last_error().
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define SA_CUDA_TRY(expr)                                   \
+  do {                                                      \
+    cudaError_t sa_e_ = (expr);                             \
+    if (sa_e_ != cudaSuccess) return ::sa::cuda_fail(sa_e_, #expr); \
+  } while (0)
+
+// Boltzmann table exactly as the reference builds it (double, glibc exp):
+// 2D src/cpu_2dp.cpp:33-40 (20 entries), 3D src/cpu_3d.cpp:99-104 (14 entries).
+void boltz_table(int lattice, double T, double h, double* out20);
+
+// u32 -> float in (0,1] used by the reference's per-site uniform draw; the
+// midpoint of bucket u (u rounded to binary32, times 2^-32, plus 2^-33).
+float uniform_from_u32(uint32_t u);
+// Number of u32 values whose uniform is below b (monotone, so u < thr(b)
+// is exactly uniform(u) < b).
+uint32_t threshold_of(float b);
+// Integer thresholds of a lattice at (T, h): float-cast table, then thr().
+// Returns false if the table is not monotone where the kernels need it.
+bool make_thresholds(int lattice, double T, double h, Thresholds* out);
+
+// Exchange decision of src/parallel_tempering.hpp:141-162 for one replica:
+// accept iff (dE*dB > 0) || r < exp(dB*dE), dE = -(E_i - E_{i+1}) as float.
+bool pt_accept(float dE, double dB, double r);
+// For h = 0 every dE is an integer in [-span, span]; the accepted set is an
+// interval [lo, hi] (possibly empty: lo > hi). Computed with the exact host
+// expression above at the boundary points.
+void pt_accept_interval(double dB, double r, int64_t span, int64_t* lo, int64_t* hi);
+
+inline int lattice_dim(int lattice) { return lattice == 2 ? 3 : 2; }
+
+}  // namespace sa

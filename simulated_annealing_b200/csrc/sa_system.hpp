@@ -1,0 +1,25 @@
+// sa_system.hpp -- the single-system handle behind sa_system_t.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "sa_device.cuh"
+
+struct sa_system {
+  int lattice = 0, dim = 2, L = 0;
+  long N = 0, half = 0, nbonds = 0;
+  double T = 1.0, h = 0.0;
+  unsigned long long seed = 1234, draw = 0, epoch = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr, own_stream = nullptr;
+  sa::word_t* d_s = nullptr;       // spins [colour][row][k]
+  sa::word_t* d_J = nullptr;       // own couplings [axis][colour][row][k]
+  sa::word_t* d_stage = nullptr;   // row-major staging for host transfers
+  unsigned long long* d_counts = nullptr;  // measure scratch (128 counters)
+  int64_t* d_EM = nullptr;         // measure output E[64], M[64]
+  sa::Thresholds thr{};
+};
+
+namespace sa {
+int launch_halfsweep(sa_system* sy, int c, unsigned long long draw);
+int launch_measure(sa_system* sy, int64_t* d_E, int64_t* d_M);
+}  // namespace sa

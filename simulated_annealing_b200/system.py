@@ -1,0 +1,175 @@
+"""GpuSystem: the reference's gpu_sys interface (src/gpu_sys.cuh:12-29) over the C ABI.
+
+Method names, argument meaning and results follow gpu_sys; the work runs in
+libsa_b200.so on the GPU. ``measure()`` returns the reference's float vector
+(index j = replica bit j); ``measure_exact()`` returns the exact integer parts.
+"""
+from __future__ import annotations
+
+import ctypes
+import struct
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+LATTICES = {"2d": _lib.SA_LATTICE_2D, "2p": _lib.SA_LATTICE_2D_OPEN_X, "3d": _lib.SA_LATTICE_3D}
+
+
+def _p(a: np.ndarray, ct=ctypes.c_uint64):
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+class GpuSystem:
+    """One lattice x 64 replicas on the GPU (gpu_2d / gpu_3d replacement)."""
+
+    def __init__(self, lattice, L: int, T: float = 1.0, h: float = 0.0):
+        if isinstance(lattice, str):
+            lattice = LATTICES[lattice]
+        self._lib = _lib.load()
+        self.lattice = int(lattice)
+        self.L = int(L)
+        self.h = float(h)
+        handle = ctypes.c_void_p()
+        check(self._lib.sa_sys_create(self.lattice, self.L, float(T), float(h), ctypes.byref(handle)))
+        self._h = handle
+        n = ctypes.c_long()
+        check(self._lib.sa_sys_get_N(self._h, ctypes.byref(n)))
+        self.N = int(n.value)
+        self.dim = 3 if self.lattice == _lib.SA_LATTICE_3D else 2
+
+    # -- gpu_sys -------------------------------------------------------------
+    def sweep(self, n: int = 1) -> None:
+        check(self._lib.sa_sys_sweep(self._h, int(n)))
+
+    def set_T(self, T: float) -> None:
+        check(self._lib.sa_sys_set_T(self._h, float(T)))
+
+    def get_T(self) -> float:
+        t = ctypes.c_double()
+        check(self._lib.sa_sys_get_T(self._h, ctypes.byref(t)))
+        return t.value
+
+    def set_h(self, h: float) -> None:
+        check(self._lib.sa_sys_set_h(self._h, float(h)))
+        self.h = float(h)
+
+    def set_seed(self, seed: int) -> None:
+        check(self._lib.sa_sys_set_seed(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF))
+
+    def measure(self) -> list[float]:
+        out = np.zeros(64, dtype=np.float32)
+        check(self._lib.sa_sys_measure_float(self._h, _p(out, ctypes.c_float)))
+        return out.tolist()
+
+    def measure_exact(self):
+        E = np.zeros(64, dtype=np.int64)
+        M = np.zeros(64, dtype=np.int64)
+        check(self._lib.sa_sys_measure(self._h, _p(E, ctypes.c_int64), _p(M, ctypes.c_int64)))
+        return E, M
+
+    def gpu_free(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.sa_sys_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def init_J(self) -> None:
+        check(self._lib.sa_sys_init_J(self._h))
+
+    def init_rand(self) -> None:
+        check(self._lib.sa_sys_init_rand(self._h))
+
+    def init_order(self) -> None:
+        check(self._lib.sa_sys_init_order(self._h))
+
+    def get_N(self) -> int:
+        return self.N
+
+    def swap(self, other: "GpuSystem", mask) -> None:
+        m = int(mask[0]) if hasattr(mask, "__len__") else int(mask)
+        check(self._lib.sa_sys_swap(self._h, other._h, m & 0xFFFFFFFFFFFFFFFF))
+
+    # J files: int dim; long N; Jx[2N]; Jy[2N]; (Jz[2N])  (src/sys_file.cpp:10-110)
+    def load_J(self, fname: str) -> None:
+        with open(fname, "rb") as f:
+            d, n = struct.unpack("<iq", f.read(12))
+            if d != self.dim:
+                raise ValueError(f"J file is {d}D, system is {self.dim}D")
+            if n != self.N:
+                raise ValueError(f"J file has N={n}, system has N={self.N}")
+            arrs = [np.frombuffer(f.read(16 * self.N), dtype=np.uint64) for _ in range(self.dim)]
+        self.set_J(*arrs)
+
+    def save_J(self, fname: str) -> None:
+        arrs = self.get_J()
+        with open(fname, "wb") as f:
+            f.write(struct.pack("<iq", self.dim, self.N))
+            for a in arrs:
+                f.write(a.astype(np.uint64).tobytes())
+
+    def save_sys(self, prefix: str) -> None:
+        """PBM image per replica bit (src/gpu_2d.cu:275-299)."""
+        s = self.get_spins()
+        rows = self.L if self.dim == 2 else self.L * self.L
+        for i in range(64):
+            bits = ((s >> np.uint64(i)) & np.uint64(1)).astype(np.uint8).reshape(rows, self.L)
+            with open(f"{prefix}{i}.pbm", "w") as f:
+                f.write(f"P1\n{self.L} {rows}\n")
+                for row in bits:
+                    f.write("".join("1 " if b else "0 " for b in row) + "\n")
+
+    def save(self) -> bytes:
+        n = ctypes.c_size_t()
+        check(self._lib.sa_sys_save(self._h, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        check(self._lib.sa_sys_save(self._h, buf, n.value, ctypes.byref(n)))
+        return buf.raw[: n.value]
+
+    def load(self, data: bytes) -> None:
+        buf = ctypes.create_string_buffer(data, len(data))
+        check(self._lib.sa_sys_load(self._h, buf, len(data)))
+
+    # -- data access -----------------------------------------------------------
+    def set_J(self, jx, jy, jz=None) -> None:
+        jx = np.ascontiguousarray(jx, dtype=np.uint64)
+        jy = np.ascontiguousarray(jy, dtype=np.uint64)
+        if self.dim == 3:
+            jz = np.ascontiguousarray(jz, dtype=np.uint64)
+            check(self._lib.sa_sys_set_J(self._h, _p(jx), _p(jy), _p(jz)))
+        else:
+            check(self._lib.sa_sys_set_J(self._h, _p(jx), _p(jy), None))
+
+    def get_J(self):
+        arrs = [np.zeros(2 * self.N, dtype=np.uint64) for _ in range(self.dim)]
+        jz = _p(arrs[2]) if self.dim == 3 else None
+        check(self._lib.sa_sys_get_J(self._h, _p(arrs[0]), _p(arrs[1]), jz))
+        return tuple(arrs)
+
+    def set_spins(self, s) -> None:
+        s = np.ascontiguousarray(s, dtype=np.uint64)
+        if s.size != self.N:
+            raise ValueError("spin array must have N words")
+        check(self._lib.sa_sys_set_spins(self._h, _p(s)))
+
+    def get_spins(self) -> np.ndarray:
+        s = np.zeros(self.N, dtype=np.uint64)
+        check(self._lib.sa_sys_get_spins(self._h, _p(s)))
+        return s
+
+    def rng_state(self):
+        a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        check(self._lib.sa_sys_get_rng(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def set_rng_state(self, seed: int, draw: int, epoch: int) -> None:
+        check(self._lib.sa_sys_set_rng(self._h, seed, draw, epoch))
+
+    def sync(self) -> None:
+        check(self._lib.sa_sys_sync(self._h))
+
+    def __del__(self):
+        try:
+            self.gpu_free()
+        except Exception:
+            pass
