@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark: replica spin-flip attempts/ns of the batched persistent engine.
+
+Workload (the batched mix): 4,096 independent +-J disorder instances, shapes
+drawn uniformly (numpy PCG64, seed 4096) from 2D L in {16,24,32,48,64} and 3D
+L in {8,12,16,20,24}, couplings and spins from seed 1000+index, 64 replicas per
+word, each a 16-temperature parallel-tempering ensemble (geometric 0.5-2.0 in
+3D, 0.3-1.6 in 2D) with an exchange attempt after every sweep. A step is one
+persistent launch of `--sweeps-per-step` sweeps over every instance. Data are
+synthetic (seeded), generated on the device from the seeds.
+
+value      attempts / device time (CUDA events on the launch stream, state
+           resident in HBM; the whole state, 1.9 GB of spins, exceeds L2).
+e2e        the same through the public API with host buffers: each step uploads
+           its exchange decisions (generated on the host by the reference's
+           std::mt19937(123) sequence) and downloads every slot's energies and
+           the acceptance counters into pinned host memory; host wall clock.
+roofline   algorithmic bytes per launch (per site and slot and sweep: spins read
+           twice and written once, 24 B; couplings 2*dim words per site, shared
+           by the 16 slots) / average launch time, against the measured HBM copy
+           bandwidth.
+cpu_baseline / --impl reference: the reference's own CPU classes (cpu_2d,
+           cpu_3d, parallel_tempering<>) compiled from its sources, on a bounded
+           sample of the same instances, timed on this host.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPES = [(0, 16), (0, 24), (0, 32), (0, 48), (0, 64), (2, 8), (2, 12), (2, 16), (2, 20), (2, 24)]
+LADDER_2D = np.geomspace(0.3, 1.6, 16)
+LADDER_3D = np.geomspace(0.5, 2.0, 16)
+METRIC = "spin-flip attempts/ns"
+UNIT = "attempts/ns"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def c4_instances(n: int, index_offset: int = 0):
+    rng = np.random.default_rng(4096)
+    picks = rng.integers(0, len(SHAPES), size=n + index_offset)[index_offset:]
+    return [(SHAPES[p][0], SHAPES[p][1], 1000 + index_offset + k) for k, p in enumerate(picks)]
+
+
+def site_count(lat: int, L: int) -> int:
+    return L ** 3 if lat == 2 else L * L
+
+
+def algorithmic_bytes_per_sweep(insts, nslots=16) -> int:
+    total = 0
+    for lat, L, _ in insts:
+        N = site_count(lat, L)
+        d = 3 if lat == 2 else 2
+        total += 24 * N * nslots + 16 * d * N
+    return total
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """dram read+write bytes per launch of the batched kernel from the committed
+    ncu summary (profiles/k_batch_c4.md, line 'traffic_bytes_per_launch: N'),
+    scaled to this run's sweeps per launch by the summary's own sweep count."""
+    p = os.path.join(ROOT, "profiles", "k_batch_c4.md")
+    try:
+        vals = {}
+        for line in open(p):
+            if ":" in line and line.strip().startswith(("traffic_bytes_per_launch", "traffic_sweeps_per_launch")):
+                k, v = line.split(":", 1)
+                vals[k.strip()] = float(v.strip().split()[0])
+        return vals.get("traffic_bytes_per_launch"), vals.get("traffic_sweeps_per_launch")
+    except Exception:
+        return None, None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        med = statistics.median(sm) if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- CPU
+def cpu_reference_sample(insts, budget_s: float, sweeps_per_instance: int = 50):
+    """The reference's parallel_tempering<cpu_sys> over cpu_2d / cpu_3d systems
+    (built as its driver builds them: set_seed; init_J; set_seed; init_rand), on
+    the first instances of the workload until `budget_s` of CPU work is done.
+    Instances run concurrently in host threads, each template using OpenMP over
+    its 16 slots, so all host cores are busy."""
+    ncpu = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(min(16, ncpu)))
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        O.build()
+    omp = int(os.environ["OMP_NUM_THREADS"])
+    workers = max(1, ncpu // max(1, omp))
+    lock = threading.Lock()
+    state = {"next": 0, "attempts": 0, "done": 0}
+    t0 = time.perf_counter()
+    deadline = t0 + budget_s
+
+    def work():
+        while True:
+            with lock:
+                if time.perf_counter() > deadline or state["next"] >= len(insts):
+                    return
+                k = state["next"]
+                state["next"] += 1
+            lat, L, seed = insts[k]
+            T = LADDER_3D if lat == 2 else LADDER_2D
+            systems = [O.RefSystem(lat, L) for _ in T]
+            for s in systems:
+                s.set_seed(seed)
+                s.init_J()
+                s.set_seed(seed)
+                s.init_rand()
+            pt = O.RefPT(systems, list(T), 1)
+            for _ in range(sweeps_per_instance):
+                pt.step(0)
+            with lock:
+                state["attempts"] += sweeps_per_instance * len(T) * site_count(lat, L) * 64
+                state["done"] += 1
+
+    threads = [threading.Thread(target=work) for _ in range(workers)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    dt = time.perf_counter() - t0
+    value = state["attempts"] / (dt * 1e9)
+    sample = (f"{state['done']} instances of the mix x 16 slots x {sweeps_per_instance} sweeps "
+              f"(+ exchange each sweep), {workers} instance threads x OMP {omp}, {dt:.1f} s")
+    return {"value": value, "unit": UNIT, "cores": min(ncpu, workers * omp), "kind": "reference",
+            "sample": sample}
+
+
+# ----------------------------------------------------------------------------- GPU
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+
+    from simulated_annealing_b200.batch import Batch
+
+    insts = c4_instances(args.instances, index_offset=rank * args.instances)
+    b = Batch()
+    l2 = b.add_ladder(LADDER_2D)
+    l3 = b.add_ladder(LADDER_3D)
+    for lat, L, seed in insts:
+        b.add_instance(lat, L, ladder=(l3 if lat == 2 else l2), seed_J=seed, seed=seed)
+    b.finalize()
+    stream = torch.cuda.Stream()
+    b.set_stream(stream.cuda_stream)
+    S = args.sweeps_per_step
+    site_slots = b.site_slots()
+    attempts_step = site_slots * 64 * S
+    n_classes = 1  # every instance has 16 slots: one persistent launch per step
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        b.run(S)
+    b.sync()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.run(S)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    barrier()
+
+    # e2e through the public API with host buffers (pinned)
+    E_host = torch.empty(b.energy_count(), dtype=torch.int64, pin_memory=True)
+    npairs = b.num_pairs()
+    acc_host = torch.empty(max(npairs, 1), dtype=torch.int64, pin_memory=True)
+    att_host = torch.empty(max(npairs, 1), dtype=torch.int64, pin_memory=True)
+    h2d = []
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        b.run(S)
+        h2d.append(b.last_h2d_bytes())
+        b.energies_into(E_host.data_ptr())
+        b.acceptance_into(acc_host.data_ptr(), att_host.data_ptr())
+        b.sync()
+    t_e2e = time.perf_counter() - t0
+    barrier()
+
+    times = torch.tensor([ms, t_e2e * 1e3], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = float(times[0]), float(times[1])
+    total_attempts = attempts_step * args.steps * world
+    value = total_attempts / (ms * 1e6)
+    e2e_value = total_attempts / (e2e_ms * 1e6)
+
+    if rank == 0:
+        peak, peak_src = measured_hbm_peak()
+        bytes_launch = algorithmic_bytes_per_sweep(insts) * S
+        launch_s = (ms / 1e3) / (args.steps * n_classes)
+        achieved = bytes_launch / launch_s / 1e9
+        tb, ts = profiled_traffic()
+        traffic = (tb * S / ts) if (tb and ts) else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64 (bitwise/int32)", "data": "synthetic",
+            "config": {"workload": "batched PT mix: 4096 instances x 16 slots, 2D L{16..64} / 3D L{8..24}, "
+                                   f"{S} sweeps + exchange per sweep per step",
+                       "instances_per_gpu": args.instances, "slots": 16, "sweeps_per_step": S,
+                       "site_slots_per_gpu": site_slots, "l2": "inputs larger than L2 (1.9 GB of spins)",
+                       "parallelism": f"instances sharded, {world} GPU(s), no collective"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(np.mean(h2d)) if h2d else 0,
+                    "d2h_bytes_per_step": int(E_host.numel() * 8 + 2 * npairs * 8)},
+            "gpu_launches": args.steps * n_classes,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
+                         else "fallback 6650 GB/s",
+                         "algorithmic_bytes_per_launch": bytes_launch},
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_reference_sample(insts, args.cpu_budget)
+        print(json.dumps(line), flush=True)
+    b.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    insts = c4_instances(args.instances)
+    per_step = []
+    samples = []
+    for k in range(args.warmup + args.steps):
+        r = cpu_reference_sample(insts[(k * 7) % len(insts):], args.ref_step_budget, sweeps_per_instance=20)
+        if k >= args.warmup:
+            per_step.append(r)
+    vals = [r["value"] for r in per_step]
+    value = float(np.mean(vals))
+    samples = per_step[-1]["sample"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": args.ref_step_budget * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64 (bitwise) + f64 compare", "data": "synthetic",
+        "config": {"workload": "batched PT mix: 4096 instances x 16 slots, 2D L{16..64} / 3D L{8..24}, "
+                               "bounded sample per step", "slots": 16},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": per_step[-1]["cores"], "kind": "reference",
+                         "sample": samples},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--sweeps-per-step", type=int, default=100)
+    ap.add_argument("--instances", type=int, default=4096)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-step-budget", type=float, default=8.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

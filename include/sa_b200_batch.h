@@ -1,0 +1,104 @@
+/*
+ * sa_b200_batch.h -- C ABI of the batched persistent engine.
+ *
+ * A batch holds many independent disorder instances of mixed shape (2D, 2D
+ * open-x, 3D; any even L), each an ensemble of `nslots` 64-replica systems
+ * sharing one coupling set -- the reference's parallel_tempering<gpu_sys>
+ * (src/parallel_tempering.hpp) over systems built the way its driver builds
+ * them (src/main_gpu.cu:251-277): set_seed(seed_J); init_J(); set_seed(seed);
+ * init_rand(); so every slot starts from the same spins and draws the same
+ * per-site Philox stream, and the slots share J.
+ *
+ * One persistent kernel advances every instance: a CTA takes an instance from
+ * a work queue and runs all requested sweeps of all its slots, with the
+ * replica exchange of src/parallel_tempering.hpp:81-115 done on the device:
+ * the exchange pair and uniform of every step come from the reference's own
+ * generator (std::mt19937(123), uniform_int_distribution<int>(0, n-2),
+ * uniform_real_distribution<double>(0,1)) on the host, converted to an exact
+ * integer accept interval for dE (valid for h = 0, which a batch requires).
+ *
+ * Anneal schedules: an instance may instead carry a temperature schedule
+ * (nslots = 1): one temperature per `sweeps_per_step` sweeps, with the running
+ * maximum of -H per replica tracked on the device (src/annealing.hpp:67-100).
+ */
+#ifndef SA_B200_BATCH_H
+#define SA_B200_BATCH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sa_batch* sa_batch_t;
+
+/* Empty batch on the current device. */
+int sa_batch_create(sa_batch_t* out);
+int sa_batch_destroy(sa_batch_t b);
+
+/* A temperature ladder (sorted ascending internally, as the PT constructor
+ * does, src/parallel_tempering.hpp:193-218). */
+int sa_batch_add_ladder(sa_batch_t b, const double* T, int n, int* ladder_id);
+/* A temperature schedule for annealing instances: T[k] holds for sweeps
+ * [k*sweeps_per_step, (k+1)*sweeps_per_step); the last entry holds after. */
+int sa_batch_add_schedule(sa_batch_t b, const double* T, int nsteps, int sweeps_per_step,
+                          int* schedule_id);
+/* An instance. Exactly one of ladder_id / schedule_id is >= 0. */
+int sa_batch_add_instance(sa_batch_t b, int lattice, int L, int ladder_id, int schedule_id,
+                          uint64_t seed_J, uint64_t seed, int* instance_id);
+/* Allocates the spin / coupling pools, generates J and the initial spins on
+ * the device and uploads the tables. No instance may be added afterwards. */
+int sa_batch_finalize(sa_batch_t b);
+
+/* Sweeps between exchange attempts (the PT template's `steps`; default 1). */
+int sa_batch_set_exchange_interval(sa_batch_t b, int sweeps_per_exchange);
+/* Anneal instances: measure every `stride` sweeps (0 = never; default 1) and
+ * fold the result into the per-replica running maximum of -H. */
+int sa_batch_set_measure_stride(sa_batch_t b, int stride);
+/* Record every exchange (pair, mask) of every PT instance, up to `capacity`
+ * exchanges per instance. */
+int sa_batch_record_exchanges(sa_batch_t b, long capacity);
+
+/* Advance every unfinished instance by up to `nsweeps` sweeps (anneal
+ * instances stop at the end of their schedule). Asynchronous on the batch's
+ * stream; the launch and its tables are prepared on the host first. */
+int sa_batch_run(sa_batch_t b, long nsweeps);
+int sa_batch_sync(sa_batch_t b);
+int sa_batch_set_stream(sa_batch_t b, void* stream);
+/* Number of sites processed per sweep over the whole batch (sum N*nslots). */
+int sa_batch_site_slots(sa_batch_t b, long long* site_slots);
+int sa_batch_num_instances(sa_batch_t b, int* n);
+
+/* Read-back (synchronous). Spins in the reference's row-major layout. */
+int sa_batch_get_spins(sa_batch_t b, int instance, int slot, uint64_t* s);
+int sa_batch_get_J(sa_batch_t b, int instance, uint64_t* jx, uint64_t* jy, uint64_t* jz);
+/* Exact E per replica bit of one slot (sum over bonds of +-1). */
+int sa_batch_measure(sa_batch_t b, int instance, int slot, int64_t* E);
+/* Accepted replica count and attempts per adjacent pair (nslots-1 each). */
+int sa_batch_acceptance(sa_batch_t b, int instance, int64_t* accepted, int64_t* attempts);
+/* Recorded exchanges of one instance: pairs[count], masks[count]. */
+int sa_batch_exchanges(sa_batch_t b, int instance, int* pairs, uint64_t* masks, long cap,
+                       long* count);
+/* Energies of every slot of every instance, into HOST memory E (pinned for
+ * speed): E[off(i) + slot*64 + j], off(i) = 64 * sum of nslots of instances
+ * before i. Asynchronous on the batch stream (sync before reading E). */
+int sa_batch_energies(sa_batch_t b, int64_t* E);
+/* Number of int64 values sa_batch_energies writes (64 * sum of nslots). */
+int sa_batch_energy_count(sa_batch_t b, long long* n);
+/* Acceptance counters of all pairs of all instances (instance-major), into
+ * host memory; asynchronous like sa_batch_energies. */
+int sa_batch_acceptance_all(sa_batch_t b, int64_t* accepted, int64_t* attempts);
+int sa_batch_num_pairs(sa_batch_t b, long long* n);
+/* Host->device bytes the last sa_batch_run copied (its exchange decisions). */
+int sa_batch_last_h2d_bytes(sa_batch_t b, long long* n);
+/* Anneal instances: running maximum of -H per replica (int64[64]) and the
+ * number of sweeps done. */
+int sa_batch_anneal_result(sa_batch_t b, int instance, int64_t* Emax, long* sweeps_done);
+/* Sweeps done by an instance so far. */
+int sa_batch_sweeps_done(sa_batch_t b, int instance, long* sweeps_done);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SA_B200_BATCH_H */

@@ -1,0 +1,1057 @@
+// sa_batch.cu -- the batched persistent engine.
+//
+// Thousands of instances (mixed 2D / 2D open-x / 3D, any even L), each an
+// ensemble of up to 32 64-replica slots sharing couplings, advance in ONE
+// persistent launch: a CTA takes an instance from a work queue and runs every
+// sweep of the launch for all its slots, then the replica exchange
+// (src/parallel_tempering.hpp:81-115) or the anneal bookkeeping
+// (src/annealing.hpp:67-100), without leaving the kernel.
+//
+// Layout per instance: spins [colour][row][k][slot] (the slot innermost, so a
+// warp's loads for a site group are contiguous), couplings [axis][colour][row][k]
+// shared by all slots. A warp maps its lanes to (site, slot) with P lanes per
+// site (P = next power of two >= nslots): the P slots of one site share the
+// coupling words (one broadcast load) and ONE Philox draw -- every slot of an
+// instance draws the same per-site stream, as the reference's slots do when its
+// driver seeds them alike (src/main_gpu.cu:262-276) -- which the warp computes
+// once per 32 sites and distributes with shuffles.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "sa_b200.h"
+#include "sa_b200_batch.h"
+#include "sa_batch.hpp"
+#include "sa_device.cuh"
+#include "sa_host.hpp"
+
+namespace sa {
+
+constexpr int kBatchThreads = 512;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int64_t kBatchMaxN = 1 << 18;  // counter width of the pair measure
+
+struct LaneThr {
+  uint32_t t[8];
+  uint32_t b[8];
+};
+
+__device__ __forceinline__ void load_thr(LaneThr& lt, const BThr* src) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    lt.t[k] = src->dn[k];
+    lt.b[k] = src->bdn[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Half-sweeps of one instance (all slots), colour c.
+// ---------------------------------------------------------------------------
+template <int P, bool OPEN_X>
+__device__ __forceinline__ void bhalf_2d(const InstDesc& d, word_t* __restrict__ S,
+                                         const word_t* __restrict__ J, int c, uint64_t draw,
+                                         const LaneThr& th) {
+  constexpr int SPS = 32 / P;  // sites per sub-step
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int L = d.L, hL = L >> 1, ns = d.nslots;
+  const long half = d.half;
+  const int slot = lane % P;
+  const bool slot_ok = slot < ns;
+  word_t* Sc = S + (long)c * half * ns;
+  const word_t* So = S + (long)(1 - c) * half * ns;
+  const word_t* Jxc = J + (long)(0 + c) * half;
+  const word_t* Jxo = J + (long)(1 - c) * half;
+  const word_t* Jyc = J + (long)(2 + c) * half;
+  const word_t* Jyo = J + (long)(3 - c) * half;
+  for (long base = (long)warp * 32; base < half; base += (long)nwarps * 32) {
+    const long my = base + lane;
+    uint32_t um = 0;
+    if (my < half) {
+      const int r = (int)(my / hL), k = (int)(my - (long)r * hL);
+      const int x = 2 * k + ((c + r) & 1);
+      um = philox_draw(d.seed, (unsigned long long)x + (unsigned long long)L * r, draw);
+    }
+#pragma unroll 1
+    for (int sub = 0; sub < P; ++sub) {
+      const int sl = sub * SPS + lane / P;
+      const uint32_t u = __shfl_sync(kFull, um, sl);
+      const long t = base + sl;
+      if (t < half && slot_ok) {
+        const int r = (int)(t / hL), k = (int)(t - (long)r * hL);
+        const int par = (c + r) & 1, x = 2 * k + par;
+        int kw, ke;
+        x_neighbours(k, par, hL, kw, ke);
+        const long rb = (long)r * hL;
+        const long rn = (long)wrap_dec(r, L) * hL, rs = (long)wrap_inc(r, L) * hL;
+        const word_t si = Sc[(rb + k) * ns + slot];
+        word_t mw = Jxc[rb + k] ^ So[(rb + kw) * ns + slot] ^ si;
+        word_t me = Jxo[rb + ke] ^ So[(rb + ke) * ns + slot] ^ si;
+        const word_t mn = Jyc[rb + k] ^ So[(rn + k) * ns + slot] ^ si;
+        const word_t ms = Jyo[rs + k] ^ So[(rs + k) * ns + slot] ^ si;
+        bool border = false;
+        if (OPEN_X) {
+          if (x == 0) { mw = ~0ULL; border = true; }
+          if (x == L - 1) { me = ~0ULL; border = true; }
+        }
+        word_t c0, c1, c2;
+        count4(mw, me, mn, ms, c0, c1, c2);
+        const uint32_t tt = (OPEN_X && border) ? prefix_count<4>(u, th.b) : prefix_count<4>(u, th.t);
+        Sc[(rb + k) * ns + slot] = si ^ ~ge_scalar(c0, c1, c2, tt);
+      }
+    }
+  }
+}
+
+template <int P>
+__device__ __forceinline__ void bhalf_3d(const InstDesc& d, word_t* __restrict__ S,
+                                         const word_t* __restrict__ J, int c, uint64_t draw,
+                                         const LaneThr& th) {
+  constexpr int SPS = 32 / P;  // columns per warp pass
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int L = d.L, hL = L >> 1, ns = d.nslots;
+  const long half = d.half;
+  const long cols = (long)L * hL;
+  const int slot = lane % P, cl = lane / P;
+  const bool slot_ok = slot < ns;
+  word_t* Sc = S + (long)c * half * ns;
+  const word_t* So = S + (long)(1 - c) * half * ns;
+  const word_t* Jxc = J + (long)(0 + c) * half;
+  const word_t* Jxo = J + (long)(1 - c) * half;
+  const word_t* Jyc = J + (long)(2 + c) * half;
+  const word_t* Jyo = J + (long)(3 - c) * half;
+  const word_t* Jzc = J + (long)(4 + c) * half;
+  const long plane = cols;  // rows*hL per z step = L*hL
+  for (long cb = (long)warp * SPS; cb < cols; cb += (long)nwarps * SPS) {
+    const long col = cb + cl;
+    const bool col_ok = col < cols;
+    const bool valid = col_ok && slot_ok;
+    const int y = col_ok ? (int)(col / hL) : 0;
+    const int k = col_ok ? (int)(col - (long)y * hL) : 0;
+    const int par = (c + y) & 1, x = 2 * k + par;
+    int kw, ke;
+    x_neighbours(k, par, hL, kw, ke);
+    const long yb = (long)y * hL, ynb = (long)wrap_dec(y, L) * hL, ysb = (long)wrap_inc(y, L) * hL;
+    word_t prev = valid ? Sc[(yb + (long)(L - 1) * plane + k) * ns + slot] : 0;
+    word_t first = 0;
+    for (int z0 = 0; z0 < L; z0 += P) {
+      const int zd = z0 + (lane % P);
+      uint32_t um = 0;
+      if (col_ok && zd < L)
+        um = philox_draw(d.seed,
+                         (unsigned long long)x + (unsigned long long)L * (unsigned long long)(y + (long)L * zd),
+                         draw);
+#pragma unroll 1
+      for (int zi = 0; zi < P; ++zi) {
+        const int z = z0 + zi;
+        if (z >= L) break;  // warp-uniform
+        const uint32_t u = __shfl_sync(kFull, um, cl * P + zi);
+        if (valid) {
+          const long zb = (long)z * plane;
+          const long zdn = (z == L - 1) ? 0 : (long)(z + 1) * plane;
+          const long idx = zb + yb + k;
+          const word_t si = Sc[idx * ns + slot];
+          const word_t sd = (z == L - 1) ? first : Sc[(zdn + yb + k) * ns + slot];
+          const word_t mw = Jxc[idx] ^ So[(zb + yb + kw) * ns + slot] ^ si;
+          const word_t me = Jxo[zb + yb + ke] ^ So[(zb + yb + ke) * ns + slot] ^ si;
+          const word_t mn = Jyc[idx] ^ So[(zb + ynb + k) * ns + slot] ^ si;
+          const word_t ms = Jyo[zb + ysb + k] ^ So[(zb + ysb + k) * ns + slot] ^ si;
+          const word_t mu = Jzc[idx] ^ prev ^ si;
+          const word_t md = Jzc[zdn + yb + k] ^ sd ^ si;
+          word_t c0, c1, c2;
+          count6(mw, me, mn, ms, mu, md, c0, c1, c2);
+          const word_t nsw = si ^ ~ge_scalar(c0, c1, c2, prefix_count<6>(u, th.t));
+          Sc[idx * ns + slot] = nsw;
+          if (z == 0) first = nsw;
+          prev = nsw;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Satisfied-bond counts per replica of slots a .. a+nsl-1 (nsl in {1,2}) into
+// cnt[q][j]; every bond counted once from its site towards -x/-y/-z.
+// ---------------------------------------------------------------------------
+__device__ void measure_slots(const InstDesc& d, const word_t* __restrict__ S,
+                              const word_t* __restrict__ J, int a, int nsl, unsigned (*cnt)[64]) {
+  for (int i = threadIdx.x; i < 128; i += blockDim.x) (&cnt[0][0])[i] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int L = d.L, hL = L >> 1, ns = d.nslots;
+  const long half = d.half, N = d.N;
+  const bool d3 = d.lattice == SA_LATTICE_3D, open = d.lattice == SA_LATTICE_2D_OPEN_X;
+  const int per = 32 / nsl;
+  const int g = lane / nsl, slot = a + lane % nsl;
+  const long plane = (long)L * hL;
+  VCount<4> sm;
+  VCount<16> big;
+  sm.clear();
+  big.clear();
+  int it = 0;
+  for (long base = (long)warp * per; base < N; base += (long)nwarps * per) {
+    const long t = base + g;
+    if (t < N) {
+      const int c = t >= half ? 1 : 0;
+      const long rem = t - (long)c * half;
+      const long r = rem / hL;
+      const int k = (int)(rem - r * hL);
+      const int y = (int)(r % L), z = (int)(r / L);
+      const int par = (c + y) & 1, x = 2 * k + par;
+      int kw, ke;
+      x_neighbours(k, par, hL, kw, ke);
+      const word_t* Sc = S + (long)c * half * ns;
+      const word_t* So = S + (long)(1 - c) * half * ns;
+      const word_t si = Sc[rem * ns + slot];
+      const long zb = (long)z * plane;
+      word_t w = (open && x == 0) ? 0 : (J[(long)(0 + c) * half + rem] ^ si ^ So[(zb + (long)y * hL + kw) * ns + slot]);
+      word_t n = J[(long)(2 + c) * half + rem] ^ si ^ So[(zb + (long)wrap_dec(y, L) * hL + k) * ns + slot];
+      word_t q0, q1;
+      if (d3) {
+        word_t u = J[(long)(4 + c) * half + rem] ^ si ^ Sc[((long)wrap_dec(z, L) * plane + (long)y * hL + k) * ns + slot];
+        q0 = w ^ n ^ u;
+        q1 = (w & n) | (u & (w ^ n));
+      } else {
+        q0 = w ^ n;
+        q1 = w & n;
+      }
+      add2_small(sm, q0, q1);
+    }
+    if (++it == 5) {  // <= 3 per site: the 4-plane counter stays below 16
+      add_small(big, sm);
+      sm.clear();
+      it = 0;
+    }
+  }
+  add_small(big, sm);
+  big.warp_sum_from(nsl);
+  const int q = lane % nsl;
+  for (int m = 0; m < 2 * nsl; ++m) {
+    const int j = (lane / nsl) + per * m;
+    atomicAdd(&cnt[q][j], big.count_of(j));
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// The persistent kernel.
+// ---------------------------------------------------------------------------
+template <int P>
+__device__ void run_instance(const BatchParams& p, const InstDesc& d, int id, unsigned (*cnt)[64],
+                             unsigned* smask) {
+  InstState* st = p.state + id;
+  uint64_t draw = st->draw;
+  int64_t sweeps = st->sweeps, xsteps = st->xsteps;
+  int64_t n = p.nsweeps;
+  if (d.sweep_limit >= 0) n = min(n, d.sweep_limit - sweeps);
+  if (n <= 0) return;
+  word_t* S = p.spins + d.spin_off;
+  const word_t* J = p.J + d.J_off;
+  const int lane = threadIdx.x & 31;
+  const int slot = lane % P;
+  LaneThr th;
+  int64_t step = -1;
+  if (d.sched < 0) load_thr(th, p.thr + d.thr_off + (slot < d.nslots ? slot : 0));
+  for (int64_t i = 0; i < n; ++i) {
+    if (d.sched >= 0) {
+      int64_t s = sweeps / d.sweeps_per_step;
+      if (s > d.thr_count - 1) s = d.thr_count - 1;
+      if (s != step) {
+        step = s;
+        load_thr(th, p.thr + d.thr_off + s);
+      }
+    }
+    for (int c = 0; c < 2; ++c) {
+      if (d.lattice == SA_LATTICE_3D) bhalf_3d<P>(d, S, J, c, draw + c, th);
+      else if (d.lattice == SA_LATTICE_2D_OPEN_X) bhalf_2d<P, true>(d, S, J, c, draw + c, th);
+      else bhalf_2d<P, false>(d, S, J, c, draw + c, th);
+      __syncthreads();
+    }
+    draw += 2;
+    const int64_t in_step = (d.sched >= 0) ? sweeps % d.sweeps_per_step : 0;
+    sweeps += 1;
+    if (d.ladder >= 0 && d.nslots > 1 && sweeps % p.xinterval == 0) {
+      const Decision dc = p.dec[d.dec_off + xsteps];
+      const int a = dc.pair;
+      measure_slots(d, S, J, a, 2, cnt);
+      if (threadIdx.x < 64) {
+        const int j = threadIdx.x;
+        const int64_t ea = 2 * (int64_t)cnt[0][j] - d.nbonds;
+        const int64_t eb = 2 * (int64_t)cnt[1][j] - d.nbonds;
+        const int64_t dE = eb - ea;
+        const bool acc = dE >= dc.lo && dE <= dc.hi;
+        const unsigned bal = __ballot_sync(kFull, acc);
+        if (lane == 0) smask[threadIdx.x >> 5] = bal;
+      }
+      __syncthreads();
+      const word_t mask = (word_t)smask[0] | ((word_t)smask[1] << 32);
+      if (mask) {
+        const int ns = d.nslots;
+        for (long t = threadIdx.x; t < d.N; t += blockDim.x) {
+          word_t* w = S + t * ns + a;
+          const word_t x0 = w[0], x1 = w[1];
+          const word_t dd = (x0 ^ x1) & mask;
+          w[0] = x0 ^ dd;
+          w[1] = x1 ^ dd;
+        }
+      }
+      if (threadIdx.x == 0) {
+        p.acc[d.pair_off + a] += __popcll(mask);
+        p.att[d.pair_off + a] += 1;
+        if (p.rec_pair && xsteps < p.rec_cap) {
+          p.rec_pair[(long)id * p.rec_cap + xsteps] = a;
+          p.rec_mask[(long)id * p.rec_cap + xsteps] = mask;
+        }
+      }
+      xsteps += 1;
+      __syncthreads();
+    }
+    if (d.sched >= 0 && p.mstride > 0 && in_step % p.mstride == 0) {
+      measure_slots(d, S, J, 0, 1, cnt);
+      if (threadIdx.x < 64) {
+        const int j = threadIdx.x;
+        const int64_t e = 2 * (int64_t)cnt[0][j] - d.nbonds;
+        const int64_t m0 = st->measured;
+        st->elast[j] = e;
+        st->emax[j] = (m0 == 0) ? e : max(st->emax[j], e);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) st->measured += 1;
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    st->draw = draw;
+    st->sweeps = sweeps;
+    st->xsteps = xsteps;
+  }
+}
+
+template <int P>
+__global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchParams p) {
+  __shared__ int s_item;
+  __shared__ unsigned s_cnt[2][64];
+  __shared__ unsigned s_mask[2];
+  __shared__ InstDesc s_d;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_item = atomicAdd(p.work, 1);
+      if (s_item < p.ninst) s_d = p.inst[p.order[s_item]];
+    }
+    __syncthreads();
+    const int item = s_item;
+    if (item >= p.ninst) break;
+    run_instance<P>(p, s_d, p.order[item], s_cnt, s_mask);
+    __syncthreads();  // s_item / s_d are reused by the next round
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Set-up kernels: couplings from seed_J (draws 0..2*dim-1, src/random.cu:25-35)
+// and spins (engine init, epoch 0) copied into every slot.
+// ---------------------------------------------------------------------------
+__global__ void k_batch_init(const InstDesc* inst, const uint64_t* seed_J, word_t* spins, word_t* J) {
+  const InstDesc d = inst[blockIdx.y];
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  const int L = d.L, hL = L >> 1, dim = d.lattice == SA_LATTICE_3D ? 3 : 2;
+  const long r = i / L;
+  const int x = (int)(i - r * L), y = (int)(r % L), c = (x + y) & 1;
+  const long rem = r * hL + (x >> 1);
+  const uint64_t sj = seed_J[blockIdx.y];
+  uint4x b0 = philox10(0, 0, (uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)sj, (uint32_t)(sj >> 32));
+  uint4x b1 = philox10(1, 0, (uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)sj, (uint32_t)(sj >> 32));
+  const uint32_t dr[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+  word_t* Jd = J + d.J_off;
+  for (int a = 0; a < dim; ++a)
+    Jd[(long)(2 * a + c) * d.half + rem] = (word_t)dr[2 * a] | ((word_t)dr[2 * a + 1] << 32);
+  uint4x s = philox10(0, 0, (uint32_t)i, 0x80000000u | (uint32_t)((uint64_t)i >> 32), (uint32_t)d.seed,
+                      (uint32_t)(d.seed >> 32));
+  const word_t w = (word_t)s.x | ((word_t)s.y << 32);
+  word_t* Sd = spins + d.spin_off + ((long)c * d.half + rem) * d.nslots;
+  for (int q = 0; q < d.nslots; ++q) Sd[q] = w;
+}
+
+__global__ void k_batch_gather(const word_t* spins, const InstDesc* inst, int id, int slot, word_t* out) {
+  const InstDesc d = inst[id];
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  const int L = d.L, hL = L >> 1;
+  const long r = i / L;
+  const int x = (int)(i - r * L), y = (int)(r % L), c = (x + y) & 1;
+  out[i] = spins[d.spin_off + ((long)c * d.half + r * hL + (x >> 1)) * d.nslots + slot];
+}
+
+__global__ void k_batch_measure_one(BatchParams p, int id, int slot, int64_t* E) {
+  __shared__ unsigned s_cnt[2][64];
+  const InstDesc d = p.inst[id];
+  measure_slots(d, p.spins + d.spin_off, p.J + d.J_off, slot, 1, s_cnt);
+  if (threadIdx.x < 64) E[threadIdx.x] = 2 * (int64_t)s_cnt[0][threadIdx.x] - d.nbonds;
+}
+
+// Energies of every slot of every instance: one block per instance, slots
+// measured two at a time; out[e_off + slot*64 + j].
+__global__ void __launch_bounds__(kBatchThreads) k_batch_energies(BatchParams p, const int64_t* e_off,
+                                                                   int64_t* out) {
+  __shared__ unsigned s_cnt[2][64];
+  const int id = blockIdx.x;
+  const InstDesc d = p.inst[id];
+  for (int a = 0; a < d.nslots; a += 2) {
+    const int nsl = (a + 1 < d.nslots) ? 2 : 1;
+    measure_slots(d, p.spins + d.spin_off, p.J + d.J_off, a, nsl, s_cnt);
+    if (threadIdx.x < 64 * nsl) {
+      const int q = threadIdx.x >> 6, j = threadIdx.x & 63;
+      out[e_off[id] + (long)(a + q) * 64 + j] = 2 * (int64_t)s_cnt[q][j] - d.nbonds;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace sa
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+using namespace sa;
+
+struct Ladder {
+  std::vector<double> T;
+  std::mt19937 gen{123};
+  std::uniform_int_distribution<int> uni_int;
+  std::uniform_real_distribution<double> uni_double{0., 1.};
+  std::vector<Decision> dec;
+  int64_t span = 0;
+  int64_t dec_off = 0;   // device segment start
+  int64_t cap = 0;       // device segment capacity
+  int64_t uploaded = 0;  // entries already on the device
+};
+
+struct Schedule {
+  std::vector<double> T;
+  int sweeps_per_step = 1;
+};
+
+struct sa_batch {
+  int device = 0;
+  bool finalized = false;
+  cudaStream_t stream = nullptr, own_stream = nullptr;
+  std::vector<Ladder> ladders;
+  std::vector<Schedule> scheds;
+  std::vector<InstDesc> inst;
+  std::vector<uint64_t> seed_J;
+  std::vector<int64_t> h_sweeps, h_xsteps;  // host mirrors of the device counters
+  int xinterval = 1, mstride = 1;
+  long rec_cap = 0;
+  int64_t site_slots = 0;
+  // device
+  InstDesc* d_inst = nullptr;
+  InstState* d_state = nullptr;
+  int32_t* d_order = nullptr;
+  int32_t* d_work = nullptr;
+  word_t* d_spins = nullptr;
+  word_t* d_J = nullptr;
+  BThr* d_thr = nullptr;
+  Decision* d_dec = nullptr;
+  int64_t dec_cap = 0;
+  int64_t* d_acc = nullptr;
+  int64_t* d_att = nullptr;
+  int32_t* d_rec_pair = nullptr;
+  uint64_t* d_rec_mask = nullptr;
+  word_t* d_stage = nullptr;
+  int64_t* d_E = nullptr;
+  int64_t npairs = 0;
+  Decision* h_dec = nullptr;  // pinned staging for decision uploads
+  int64_t h_dec_cap = 0;
+  int64_t h2d_bytes_last = 0;  // host->device bytes of the last sa_batch_run
+  int64_t* d_Eall = nullptr;   // all-slot energies
+  int64_t e_count = 0;         // sum of nslots*64
+  // work classes by lanes-per-site P = 1,2,4,8,16,32: a contiguous range of
+  // the work order each, one persistent launch per non-empty class
+  int cls_begin[6] = {0, 0, 0, 0, 0, 0};
+  int cls_count[6] = {0, 0, 0, 0, 0, 0};
+  int cls_grid[6] = {0, 0, 0, 0, 0, 0};
+};
+
+static int p_class(int P) {
+  int c = 0;
+  while ((1 << c) < P) ++c;
+  return c;
+}
+
+template <int P>
+static void launch_class(sa_batch* b, int cls, long nsweeps);
+
+static BThr to_bthr(int lattice, double T) {
+  Thresholds t;
+  make_thresholds(lattice, T, 0.0, &t);
+  BThr b;
+  memcpy(b.dn, t.dn, sizeof b.dn);
+  memcpy(b.bdn, t.bdn, sizeof b.bdn);
+  return b;
+}
+
+static int batch_params(sa_batch* b, long nsweeps, BatchParams* p) {
+  p->inst = b->d_inst;
+  p->state = b->d_state;
+  p->order = b->d_order;
+  p->ninst = (int32_t)b->inst.size();
+  p->work = b->d_work;
+  p->spins = b->d_spins;
+  p->J = b->d_J;
+  p->thr = b->d_thr;
+  p->dec = b->d_dec;
+  p->acc = b->d_acc;
+  p->att = b->d_att;
+  p->rec_pair = b->d_rec_pair;
+  p->rec_mask = b->d_rec_mask;
+  p->rec_cap = b->rec_cap;
+  p->nsweeps = nsweeps;
+  p->xinterval = b->xinterval;
+  p->mstride = b->mstride;
+  return SA_OK;
+}
+
+// Extends every ladder's exchange table to cover `need` attempts. Each
+// ladder owns a device segment with room for `cap` entries; new entries are
+// copied host->device as they are generated (only the new ones), and a
+// segment that runs out of room is reallocated with double the capacity.
+static int ensure_decisions(sa_batch* b, const std::vector<int64_t>& need) {
+  bool relayout = (b->d_dec == nullptr);
+  for (size_t l = 0; l < b->ladders.size(); ++l) {
+    Ladder& ld = b->ladders[l];
+    while ((int64_t)ld.dec.size() < need[l]) {
+      Decision dc;
+      int i = ld.uni_int(ld.gen);         // src/parallel_tempering.hpp:112
+      double r = ld.uni_double(ld.gen);   // src/parallel_tempering.hpp:114
+      double dB = (1. / ld.T[i] - 1. / ld.T[i + 1]);
+      int64_t lo, hi;
+      pt_accept_interval(dB, r, ld.span, &lo, &hi);
+      dc.pair = i;
+      dc.lo = (int32_t)std::max<int64_t>(lo, -2147483647LL);
+      dc.hi = (int32_t)std::min<int64_t>(hi, 2147483647LL);
+      dc.pad = 0;
+      ld.dec.push_back(dc);
+    }
+    if ((int64_t)ld.dec.size() > ld.cap) relayout = true;
+  }
+  if (relayout) {
+    int64_t total = 0;
+    for (Ladder& ld : b->ladders) {
+      ld.cap = std::max<int64_t>(1024, 2 * (int64_t)ld.dec.size());
+      ld.dec_off = total;
+      ld.uploaded = 0;
+      total += ld.cap;
+    }
+    SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    cudaFree(b->d_dec);
+    b->d_dec = nullptr;
+    SA_CUDA_TRY(cudaMalloc(&b->d_dec, std::max<int64_t>(total, 1) * sizeof(Decision)));
+    b->dec_cap = total;
+    for (InstDesc& d : b->inst)
+      if (d.ladder >= 0) d.dec_off = b->ladders[d.ladder].dec_off;
+    SA_CUDA_TRY(cudaMemcpyAsync(b->d_inst, b->inst.data(), b->inst.size() * sizeof(InstDesc),
+                                cudaMemcpyHostToDevice, b->stream));
+  }
+  // stage the new entries in pinned memory and copy them after the previous ones
+  int64_t fresh = 0;
+  for (Ladder& ld : b->ladders) fresh += (int64_t)ld.dec.size() - ld.uploaded;
+  if (fresh == 0) return SA_OK;
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));  // the pinned staging buffer is reused
+  if (fresh > b->h_dec_cap) {
+    if (b->h_dec) cudaFreeHost(b->h_dec);
+    b->h_dec = nullptr;
+    b->h_dec_cap = std::max<int64_t>(fresh, 4096);
+    SA_CUDA_TRY(cudaHostAlloc((void**)&b->h_dec, b->h_dec_cap * sizeof(Decision), cudaHostAllocDefault));
+  }
+  int64_t pos = 0;
+  for (Ladder& ld : b->ladders) {
+    const int64_t n = (int64_t)ld.dec.size() - ld.uploaded;
+    if (n <= 0) continue;
+    memcpy(b->h_dec + pos, ld.dec.data() + ld.uploaded, n * sizeof(Decision));
+    SA_CUDA_TRY(cudaMemcpyAsync(b->d_dec + ld.dec_off + ld.uploaded, b->h_dec + pos, n * sizeof(Decision),
+                                cudaMemcpyHostToDevice, b->stream));
+    b->h2d_bytes_last += n * (int64_t)sizeof(Decision);
+    ld.uploaded += n;
+    pos += n;
+  }
+  return SA_OK;
+}
+
+template <int P>
+static void launch_class(sa_batch* b, int cls, long nsweeps) {
+  BatchParams p;
+  batch_params(b, nsweeps, &p);
+  p.order = b->d_order + b->cls_begin[cls];
+  p.ninst = b->cls_count[cls];
+  p.work = b->d_work + cls;
+  k_batch<P><<<b->cls_grid[cls], kBatchThreads, 0, b->stream>>>(p);
+}
+
+extern "C" {
+
+int sa_batch_create(sa_batch_t* out) {
+  if (!out) return fail(SA_ERR_INVALID, "out is null");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(SA_ERR_NO_DEVICE, "no CUDA device available");
+  sa_batch* b = new sa_batch();
+  cudaGetDevice(&b->device);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete b;
+    return cuda_fail(e, "cudaStreamCreate");
+  }
+  b->stream = b->own_stream;
+  *out = b;
+  return SA_OK;
+}
+
+int sa_batch_destroy(sa_batch_t b) {
+  if (!b) return SA_OK;
+  cudaStreamSynchronize(b->stream);
+  cudaFree(b->d_inst);
+  cudaFree(b->d_state);
+  cudaFree(b->d_order);
+  cudaFree(b->d_work);
+  cudaFree(b->d_spins);
+  cudaFree(b->d_J);
+  cudaFree(b->d_thr);
+  cudaFree(b->d_dec);
+  cudaFree(b->d_acc);
+  cudaFree(b->d_att);
+  cudaFree(b->d_rec_pair);
+  cudaFree(b->d_rec_mask);
+  cudaFree(b->d_stage);
+  cudaFree(b->d_E);
+  cudaFree(b->d_Eall);
+  if (b->h_dec) cudaFreeHost(b->h_dec);
+  if (b->own_stream) cudaStreamDestroy(b->own_stream);
+  delete b;
+  return SA_OK;
+}
+
+int sa_batch_add_ladder(sa_batch_t b, const double* T, int n, int* id) {
+  if (!b || !T || !id) return fail(SA_ERR_INVALID, "null argument");
+  if (b->finalized) return fail(SA_ERR_INVALID, "batch already finalized");
+  if (n < 1 || n > 32) return fail(SA_ERR_UNSUPPORTED, "a ladder holds 1..32 temperatures");
+  Ladder ld;
+  ld.T.assign(T, T + n);
+  for (double t : ld.T)
+    if (!(t > 0)) return fail(SA_ERR_INVALID, "temperatures must be > 0");
+  std::sort(ld.T.begin(), ld.T.end());
+  ld.uni_int = std::uniform_int_distribution<int>(0, std::max(0, n - 2));
+  b->ladders.push_back(ld);
+  *id = (int)b->ladders.size() - 1;
+  return SA_OK;
+}
+
+int sa_batch_add_schedule(sa_batch_t b, const double* T, int nsteps, int sweeps_per_step, int* id) {
+  if (!b || !T || !id) return fail(SA_ERR_INVALID, "null argument");
+  if (b->finalized) return fail(SA_ERR_INVALID, "batch already finalized");
+  if (nsteps < 1 || sweeps_per_step < 1) return fail(SA_ERR_INVALID, "empty schedule");
+  Schedule s;
+  s.T.assign(T, T + nsteps);
+  for (double t : s.T)
+    if (!(t > 0)) return fail(SA_ERR_INVALID, "temperatures must be > 0");
+  s.sweeps_per_step = sweeps_per_step;
+  b->scheds.push_back(s);
+  *id = (int)b->scheds.size() - 1;
+  return SA_OK;
+}
+
+int sa_batch_add_instance(sa_batch_t b, int lattice, int L, int ladder, int sched, uint64_t seed_J,
+                          uint64_t seed, int* id) {
+  if (!b || !id) return fail(SA_ERR_INVALID, "null argument");
+  if (b->finalized) return fail(SA_ERR_INVALID, "batch already finalized");
+  if (lattice < 0 || lattice > 2) return fail(SA_ERR_INVALID, "unknown lattice kind");
+  if (L < 2) return fail(SA_ERR_INVALID, "L must be >= 2");
+  if (L & 1) return fail(SA_ERR_ODD_L, "L must be even");
+  if ((ladder >= 0) == (sched >= 0)) return fail(SA_ERR_INVALID, "exactly one of ladder / schedule");
+  if (ladder >= (int)b->ladders.size() || sched >= (int)b->scheds.size())
+    return fail(SA_ERR_INVALID, "unknown ladder / schedule id");
+  InstDesc d;
+  memset(&d, 0, sizeof d);
+  const int dim = lattice_dim(lattice);
+  d.lattice = lattice;
+  d.L = L;
+  d.N = (dim == 3) ? (int64_t)L * L * L : (int64_t)L * L;
+  if (d.N > kBatchMaxN) return fail(SA_ERR_UNSUPPORTED, "instance too large for the batched engine");
+  d.half = d.N / 2;
+  d.nbonds = dim * d.N - (lattice == SA_LATTICE_2D_OPEN_X ? L : 0);
+  d.ladder = ladder;
+  d.sched = sched;
+  d.nslots = (ladder >= 0) ? (int)b->ladders[ladder].T.size() : 1;
+  int P = 1;
+  while (P < d.nslots) P <<= 1;
+  d.P = P;
+  d.seed = seed;
+  if (sched >= 0) {
+    d.sweeps_per_step = b->scheds[sched].sweeps_per_step;
+    d.thr_count = (int)b->scheds[sched].T.size();
+    d.sweep_limit = (int64_t)d.thr_count * d.sweeps_per_step;
+  } else {
+    d.sweeps_per_step = 1;
+    d.sweep_limit = -1;
+    Ladder& ld = b->ladders[ladder];
+    ld.span = std::max<int64_t>(ld.span, 2 * d.nbonds);
+  }
+  b->inst.push_back(d);
+  b->seed_J.push_back(seed_J);
+  *id = (int)b->inst.size() - 1;
+  return SA_OK;
+}
+
+int sa_batch_finalize(sa_batch_t b) {
+  if (!b) return fail(SA_ERR_INVALID, "null batch");
+  if (b->finalized) return SA_OK;
+  if (b->inst.empty()) return fail(SA_ERR_INVALID, "empty batch");
+  // offsets and threshold pool: one block per (ladder or schedule, lattice kind)
+  std::map<std::pair<int, int>, int64_t> thr_at;  // key (+ladder+1 or -(sched+1), lattice)
+  std::vector<BThr> thr;
+  int64_t spin_off = 0, J_off = 0, pair_off = 0;
+  b->site_slots = 0;
+  for (InstDesc& d : b->inst) {
+    const int dim = lattice_dim(d.lattice);
+    d.spin_off = spin_off;
+    spin_off += d.N * d.nslots;
+    d.J_off = J_off;
+    J_off += dim * d.N;
+    d.pair_off = pair_off;
+    pair_off += std::max(0, d.nslots - 1);
+    b->site_slots += d.N * d.nslots;
+    auto key = std::make_pair(d.ladder >= 0 ? d.ladder + 1 : -(d.sched + 1), d.lattice);
+    auto it = thr_at.find(key);
+    if (it == thr_at.end()) {
+      int64_t off = (int64_t)thr.size();
+      const std::vector<double>& Ts = d.ladder >= 0 ? b->ladders[d.ladder].T : b->scheds[d.sched].T;
+      for (double t : Ts) thr.push_back(to_bthr(d.lattice, t));
+      it = thr_at.emplace(key, off).first;
+    }
+    d.thr_off = it->second;
+  }
+  b->npairs = pair_off;
+  // work order: grouped by P class, most expensive first inside a class
+  std::vector<int32_t> order(b->inst.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int32_t)i;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+    const InstDesc &dx = b->inst[x], &dy = b->inst[y];
+    if (dx.P != dy.P) return dx.P < dy.P;
+    return dx.N * dx.nslots > dy.N * dy.nslots;
+  });
+  for (size_t i = 0; i < order.size(); ++i) {
+    const int c = p_class(b->inst[order[i]].P);
+    if (b->cls_count[c] == 0) b->cls_begin[c] = (int)i;
+    b->cls_count[c] += 1;
+  }
+  const size_t ni = b->inst.size();
+  SA_CUDA_TRY(cudaMalloc(&b->d_inst, ni * sizeof(InstDesc)));
+  SA_CUDA_TRY(cudaMalloc(&b->d_state, ni * sizeof(InstState)));
+  SA_CUDA_TRY(cudaMalloc(&b->d_order, ni * sizeof(int32_t)));
+  SA_CUDA_TRY(cudaMalloc(&b->d_work, 6 * sizeof(int32_t)));
+  SA_CUDA_TRY(cudaMalloc(&b->d_spins, std::max<int64_t>(spin_off, 1) * sizeof(word_t)));
+  SA_CUDA_TRY(cudaMalloc(&b->d_J, std::max<int64_t>(J_off, 1) * sizeof(word_t)));
+  SA_CUDA_TRY(cudaMalloc(&b->d_thr, std::max<size_t>(thr.size(), 1) * sizeof(BThr)));
+  SA_CUDA_TRY(cudaMalloc(&b->d_acc, std::max<int64_t>(pair_off, 1) * sizeof(int64_t)));
+  SA_CUDA_TRY(cudaMalloc(&b->d_att, std::max<int64_t>(pair_off, 1) * sizeof(int64_t)));
+  SA_CUDA_TRY(cudaMalloc(&b->d_E, 64 * sizeof(int64_t)));
+  int64_t maxN = 0;
+  for (const InstDesc& d : b->inst) maxN = std::max(maxN, d.N);
+  SA_CUDA_TRY(cudaMalloc(&b->d_stage, maxN * sizeof(word_t)));
+  SA_CUDA_TRY(cudaMemsetAsync(b->d_state, 0, ni * sizeof(InstState), b->stream));
+  SA_CUDA_TRY(cudaMemsetAsync(b->d_acc, 0, std::max<int64_t>(pair_off, 1) * sizeof(int64_t), b->stream));
+  SA_CUDA_TRY(cudaMemsetAsync(b->d_att, 0, std::max<int64_t>(pair_off, 1) * sizeof(int64_t), b->stream));
+  SA_CUDA_TRY(cudaMemcpyAsync(b->d_order, order.data(), ni * sizeof(int32_t), cudaMemcpyHostToDevice, b->stream));
+  if (!thr.empty())
+    SA_CUDA_TRY(cudaMemcpyAsync(b->d_thr, thr.data(), thr.size() * sizeof(BThr), cudaMemcpyHostToDevice, b->stream));
+  SA_CUDA_TRY(cudaMemcpyAsync(b->d_inst, b->inst.data(), ni * sizeof(InstDesc), cudaMemcpyHostToDevice, b->stream));
+  uint64_t* d_seedJ = nullptr;
+  SA_CUDA_TRY(cudaMalloc(&d_seedJ, ni * sizeof(uint64_t)));
+  SA_CUDA_TRY(cudaMemcpyAsync(d_seedJ, b->seed_J.data(), ni * sizeof(uint64_t), cudaMemcpyHostToDevice, b->stream));
+  dim3 g((unsigned)((maxN + 255) / 256), (unsigned)ni);
+  k_batch_init<<<g, 256, 0, b->stream>>>(b->d_inst, d_seedJ, b->d_spins, b->d_J);
+  SA_CUDA_TRY(cudaGetLastError());
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  cudaFree(d_seedJ);
+  b->h_sweeps.assign(ni, 0);
+  b->h_xsteps.assign(ni, 0);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  const void* kernels[6] = {(const void*)k_batch<1>, (const void*)k_batch<2>, (const void*)k_batch<4>,
+                            (const void*)k_batch<8>, (const void*)k_batch<16>, (const void*)k_batch<32>};
+  for (int c = 0; c < 6; ++c) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernels[c], kBatchThreads, 0);
+    if (per_sm < 1) per_sm = 1;
+    b->cls_grid[c] = (int)std::min<int64_t>((int64_t)sms * per_sm, (int64_t)b->cls_count[c]);
+  }
+  b->finalized = true;
+  // the ladders' first exchanges
+  std::vector<int64_t> need(b->ladders.size(), 1);
+  return ensure_decisions(b, need);
+}
+
+int sa_batch_set_exchange_interval(sa_batch_t b, int k) {
+  if (!b || k < 1) return fail(SA_ERR_INVALID, "interval must be >= 1");
+  b->xinterval = k;
+  return SA_OK;
+}
+
+int sa_batch_set_measure_stride(sa_batch_t b, int stride) {
+  if (!b || stride < 0) return fail(SA_ERR_INVALID, "stride must be >= 0");
+  b->mstride = stride;
+  return SA_OK;
+}
+
+int sa_batch_record_exchanges(sa_batch_t b, long cap) {
+  if (!b || cap < 0) return fail(SA_ERR_INVALID, "bad capacity");
+  if (!b->finalized) return fail(SA_ERR_INVALID, "finalize the batch first");
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  cudaFree(b->d_rec_pair);
+  cudaFree(b->d_rec_mask);
+  b->d_rec_pair = nullptr;
+  b->d_rec_mask = nullptr;
+  b->rec_cap = cap;
+  if (cap > 0) {
+    size_t n = (size_t)cap * b->inst.size();
+    SA_CUDA_TRY(cudaMalloc(&b->d_rec_pair, n * sizeof(int32_t)));
+    SA_CUDA_TRY(cudaMalloc(&b->d_rec_mask, n * sizeof(uint64_t)));
+    SA_CUDA_TRY(cudaMemset(b->d_rec_pair, 0xFF, n * sizeof(int32_t)));
+    SA_CUDA_TRY(cudaMemset(b->d_rec_mask, 0, n * sizeof(uint64_t)));
+  }
+  return SA_OK;
+}
+
+int sa_batch_run(sa_batch_t b, long nsweeps) {
+  if (!b) return fail(SA_ERR_INVALID, "null batch");
+  if (!b->finalized) return fail(SA_ERR_INVALID, "finalize the batch first");
+  if (nsweeps < 0) return fail(SA_ERR_INVALID, "nsweeps < 0");
+  if (nsweeps == 0) return SA_OK;
+  // host mirror of the counters -> exchange-table lengths this launch needs
+  std::vector<int64_t> need(b->ladders.size(), 0);
+  for (size_t i = 0; i < b->inst.size(); ++i) {
+    const InstDesc& d = b->inst[i];
+    int64_t n = nsweeps;
+    if (d.sweep_limit >= 0) n = std::max<int64_t>(0, std::min<int64_t>(n, d.sweep_limit - b->h_sweeps[i]));
+    const int64_t s1 = b->h_sweeps[i] + n;
+    if (d.ladder >= 0 && d.nslots > 1) {
+      const int64_t x1 = s1 / b->xinterval;
+      b->h_xsteps[i] = x1;
+      need[d.ladder] = std::max(need[d.ladder], x1);
+    }
+    b->h_sweeps[i] = s1;
+  }
+  b->h2d_bytes_last = 0;
+  int st = ensure_decisions(b, need);
+  if (st) return st;
+  SA_CUDA_TRY(cudaMemsetAsync(b->d_work, 0, 6 * sizeof(int32_t), b->stream));
+  if (b->cls_count[0]) launch_class<1>(b, 0, nsweeps);
+  if (b->cls_count[1]) launch_class<2>(b, 1, nsweeps);
+  if (b->cls_count[2]) launch_class<4>(b, 2, nsweeps);
+  if (b->cls_count[3]) launch_class<8>(b, 3, nsweeps);
+  if (b->cls_count[4]) launch_class<16>(b, 4, nsweeps);
+  if (b->cls_count[5]) launch_class<32>(b, 5, nsweeps);
+  SA_CUDA_TRY(cudaGetLastError());
+  return SA_OK;
+}
+
+int sa_batch_sync(sa_batch_t b) {
+  if (!b) return fail(SA_ERR_INVALID, "null batch");
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return SA_OK;
+}
+
+int sa_batch_set_stream(sa_batch_t b, void* stream) {
+  if (!b) return fail(SA_ERR_INVALID, "null batch");
+  b->stream = stream ? (cudaStream_t)stream : b->own_stream;
+  return SA_OK;
+}
+
+int sa_batch_site_slots(sa_batch_t b, long long* n) {
+  if (!b || !n) return fail(SA_ERR_INVALID, "null argument");
+  long long s = 0;
+  for (const InstDesc& d : b->inst) s += d.N * d.nslots;
+  *n = s;
+  return SA_OK;
+}
+
+int sa_batch_num_instances(sa_batch_t b, int* n) {
+  if (!b || !n) return fail(SA_ERR_INVALID, "null argument");
+  *n = (int)b->inst.size();
+  return SA_OK;
+}
+
+static int check_inst(sa_batch* b, int id) {
+  if (!b) return fail(SA_ERR_INVALID, "null batch");
+  if (!b->finalized) return fail(SA_ERR_INVALID, "finalize the batch first");
+  if (id < 0 || id >= (int)b->inst.size()) return fail(SA_ERR_INVALID, "instance id out of range");
+  return SA_OK;
+}
+
+int sa_batch_get_spins(sa_batch_t b, int id, int slot, uint64_t* s) {
+  int st = check_inst(b, id);
+  if (st) return st;
+  const InstDesc& d = b->inst[id];
+  if (!s || slot < 0 || slot >= d.nslots) return fail(SA_ERR_INVALID, "bad slot / buffer");
+  k_batch_gather<<<(unsigned)((d.N + 255) / 256), 256, 0, b->stream>>>(b->d_spins, b->d_inst, id, slot,
+                                                                       b->d_stage);
+  SA_CUDA_TRY(cudaGetLastError());
+  SA_CUDA_TRY(cudaMemcpyAsync(s, b->d_stage, d.N * sizeof(word_t), cudaMemcpyDeviceToHost, b->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return SA_OK;
+}
+
+int sa_batch_get_J(sa_batch_t b, int id, uint64_t* jx, uint64_t* jy, uint64_t* jz) {
+  int st = check_inst(b, id);
+  if (st) return st;
+  const InstDesc& d = b->inst[id];
+  const int dim = lattice_dim(d.lattice);
+  if (!jx || !jy || (dim == 3 && !jz)) return fail(SA_ERR_INVALID, "null buffer");
+  std::vector<word_t> own(dim * d.N);
+  SA_CUDA_TRY(cudaMemcpyAsync(own.data(), b->d_J + d.J_off, own.size() * sizeof(word_t), cudaMemcpyDeviceToHost,
+                              b->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  const long L = d.L, L2 = L * L, N = d.N, hL = L / 2;
+  auto split = [&](long i) {
+    long r = i / L;
+    int x = (int)(i - r * L), y = (int)(r % L), c = (x + y) & 1;
+    return (long)c * d.half + r * hL + (x >> 1);
+  };
+  for (long i = 0; i < N; ++i) {
+    long e = ((i + 1) % L == 0) ? i - L + 1 : i + 1;
+    long s_ = ((i + L) % L2 < L) ? i - L2 + L : i + L;
+    jx[2 * i] = own[split(i)];
+    jx[2 * i + 1] = own[split(e)];
+    jy[2 * i] = own[N + split(i)];
+    jy[2 * i + 1] = own[N + split(s_)];
+    if (dim == 3) {
+      long dd = (i + L2 >= N) ? i - N + L2 : i + L2;
+      jz[2 * i] = own[2 * N + split(i)];
+      jz[2 * i + 1] = own[2 * N + split(dd)];
+    }
+  }
+  return SA_OK;
+}
+
+int sa_batch_measure(sa_batch_t b, int id, int slot, int64_t* E) {
+  int st = check_inst(b, id);
+  if (st) return st;
+  if (!E || slot < 0 || slot >= b->inst[id].nslots) return fail(SA_ERR_INVALID, "bad slot / buffer");
+  BatchParams p;
+  batch_params(b, 0, &p);
+  k_batch_measure_one<<<1, kBatchThreads, 0, b->stream>>>(p, id, slot, b->d_E);
+  SA_CUDA_TRY(cudaGetLastError());
+  SA_CUDA_TRY(cudaMemcpyAsync(E, b->d_E, 64 * sizeof(int64_t), cudaMemcpyDeviceToHost, b->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return SA_OK;
+}
+
+int sa_batch_acceptance(sa_batch_t b, int id, int64_t* accepted, int64_t* attempts) {
+  int st = check_inst(b, id);
+  if (st) return st;
+  const InstDesc& d = b->inst[id];
+  const int np = std::max(0, d.nslots - 1);
+  if (np == 0) return SA_OK;
+  if (!accepted || !attempts) return fail(SA_ERR_INVALID, "null buffer");
+  SA_CUDA_TRY(cudaMemcpyAsync(accepted, b->d_acc + d.pair_off, np * sizeof(int64_t), cudaMemcpyDeviceToHost, b->stream));
+  SA_CUDA_TRY(cudaMemcpyAsync(attempts, b->d_att + d.pair_off, np * sizeof(int64_t), cudaMemcpyDeviceToHost, b->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return SA_OK;
+}
+
+int sa_batch_exchanges(sa_batch_t b, int id, int* pairs, uint64_t* masks, long cap, long* count) {
+  int st = check_inst(b, id);
+  if (st) return st;
+  if (!count) return fail(SA_ERR_INVALID, "null count");
+  long n = std::min<long>((long)b->h_xsteps[id], b->rec_cap);
+  *count = n;
+  if (!pairs || !masks || n == 0) return SA_OK;
+  if (cap < n) return fail(SA_ERR_BUFFER, "buffer smaller than the recorded exchanges");
+  SA_CUDA_TRY(cudaMemcpyAsync(pairs, b->d_rec_pair + (long)id * b->rec_cap, n * sizeof(int32_t),
+                              cudaMemcpyDeviceToHost, b->stream));
+  SA_CUDA_TRY(cudaMemcpyAsync(masks, b->d_rec_mask + (long)id * b->rec_cap, n * sizeof(uint64_t),
+                              cudaMemcpyDeviceToHost, b->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return SA_OK;
+}
+
+int sa_batch_energies(sa_batch_t b, int64_t* E) {
+  if (!b || !E) return fail(SA_ERR_INVALID, "null argument");
+  if (!b->finalized) return fail(SA_ERR_INVALID, "finalize the batch first");
+  if (!b->d_Eall) {
+    std::vector<int64_t> off(b->inst.size());
+    int64_t o = 0;
+    for (size_t i = 0; i < b->inst.size(); ++i) {
+      off[i] = o;
+      o += (int64_t)b->inst[i].nslots * 64;
+    }
+    b->e_count = o;
+    SA_CUDA_TRY(cudaMalloc(&b->d_Eall, (o + (int64_t)off.size()) * sizeof(int64_t)));
+    SA_CUDA_TRY(cudaMemcpy(b->d_Eall + o, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  }
+  BatchParams p;
+  batch_params(b, 0, &p);
+  k_batch_energies<<<(unsigned)b->inst.size(), kBatchThreads, 0, b->stream>>>(p, b->d_Eall + b->e_count,
+                                                                                b->d_Eall);
+  SA_CUDA_TRY(cudaGetLastError());
+  SA_CUDA_TRY(cudaMemcpyAsync(E, b->d_Eall, b->e_count * sizeof(int64_t), cudaMemcpyDeviceToHost, b->stream));
+  return SA_OK;
+}
+
+int sa_batch_energy_count(sa_batch_t b, long long* n) {
+  if (!b || !n) return fail(SA_ERR_INVALID, "null argument");
+  long long o = 0;
+  for (const InstDesc& d : b->inst) o += (long long)d.nslots * 64;
+  *n = o;
+  return SA_OK;
+}
+
+int sa_batch_last_h2d_bytes(sa_batch_t b, long long* n) {
+  if (!b || !n) return fail(SA_ERR_INVALID, "null argument");
+  *n = b->h2d_bytes_last;
+  return SA_OK;
+}
+
+int sa_batch_acceptance_all(sa_batch_t b, int64_t* accepted, int64_t* attempts) {
+  if (!b || !accepted || !attempts) return fail(SA_ERR_INVALID, "null argument");
+  if (!b->finalized) return fail(SA_ERR_INVALID, "finalize the batch first");
+  if (b->npairs == 0) return SA_OK;
+  SA_CUDA_TRY(cudaMemcpyAsync(accepted, b->d_acc, b->npairs * sizeof(int64_t), cudaMemcpyDeviceToHost, b->stream));
+  SA_CUDA_TRY(cudaMemcpyAsync(attempts, b->d_att, b->npairs * sizeof(int64_t), cudaMemcpyDeviceToHost, b->stream));
+  return SA_OK;
+}
+
+int sa_batch_num_pairs(sa_batch_t b, long long* n) {
+  if (!b || !n) return fail(SA_ERR_INVALID, "null argument");
+  *n = b->npairs;
+  return SA_OK;
+}
+
+int sa_batch_anneal_result(sa_batch_t b, int id, int64_t* Emax, long* sweeps_done) {
+  int st = check_inst(b, id);
+  if (st) return st;
+  InstState s;
+  SA_CUDA_TRY(cudaMemcpyAsync(&s, b->d_state + id, sizeof s, cudaMemcpyDeviceToHost, b->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  if (Emax) memcpy(Emax, s.emax, sizeof s.emax);
+  if (sweeps_done) *sweeps_done = (long)s.sweeps;
+  return SA_OK;
+}
+
+int sa_batch_sweeps_done(sa_batch_t b, int id, long* sweeps_done) {
+  int st = check_inst(b, id);
+  if (st) return st;
+  if (!sweeps_done) return fail(SA_ERR_INVALID, "null argument");
+  InstState s;
+  SA_CUDA_TRY(cudaMemcpyAsync(&s, b->d_state + id, sizeof s, cudaMemcpyDeviceToHost, b->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  *sweeps_done = (long)s.sweeps;
+  return SA_OK;
+}
+
+}  // extern "C"

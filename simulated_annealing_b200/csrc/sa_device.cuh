@@ -12,9 +12,9 @@
 #pragma once
 #include <cstdint>
 
-namespace sa {
+#include "sa_types.hpp"
 
-typedef unsigned long long word_t;
+namespace sa {
 
 // ---------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11). Stream (key = seed,
@@ -65,13 +65,6 @@ __device__ __forceinline__ uint32_t philox_draw(unsigned long long seed, unsigne
 // accepted k form a prefix and "accept" is "k < t(u)" with
 // t(u) = #{k : u < thr[k]}.
 // ---------------------------------------------------------------------------
-struct Thresholds {
-  uint32_t dn[8];   // spin down (bit 0): boltz[0..z]
-  uint32_t up[8];   // spin up   (bit 1): boltz[z+1..2z+1]
-  uint32_t bdn[8];  // open-x border sites, spin down: boltz[10..14]
-  uint32_t bup[8];  // open-x border sites, spin up:   boltz[15..19]
-};
-
 template <int NB>
 __device__ __forceinline__ uint32_t prefix_count(uint32_t u, const uint32_t* thr) {
   uint32_t t = 0;
@@ -140,6 +133,82 @@ __device__ __forceinline__ int wrap_inc(int v, int n) { return v == n - 1 ? 0 : 
 __device__ __forceinline__ void x_neighbours(int k, int par, int half_L, int& kw, int& ke) {
   if (par == 0) { kw = wrap_dec(k, half_L); ke = k; }
   else { kw = k; ke = wrap_inc(k, half_L); }
+}
+
+// Bit-sliced vertical counter: plane b holds bit b of 64 per-replica counts.
+template <int B>
+struct VCount {
+  word_t p[B];
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int b = 0; b < B; ++b) p[b] = 0;
+  }
+  __device__ __forceinline__ void add(word_t m) {
+    word_t carry = m;
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      word_t t = p[b] & carry;
+      p[b] ^= carry;
+      carry = t;
+    }
+  }
+  __device__ __forceinline__ void add_counter(const VCount& o) {
+    word_t carry = 0;
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      word_t a = p[b], q = o.p[b];
+      p[b] = a ^ q ^ carry;
+      carry = (a & q) | (carry & (a ^ q));
+    }
+  }
+  // Sum over the lanes of a warp (result valid in every lane).
+  __device__ __forceinline__ void warp_sum() { warp_sum_from(1); }
+  // Sum over the lanes that share (lane mod first_off); first_off a power of
+  // 2. Ripple-carry, fetching the partner's plane just before it is added.
+  __device__ __forceinline__ void warp_sum_from(int first_off) {
+    for (int off = 16; off >= first_off; off >>= 1) {
+      word_t carry = 0;
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const word_t a = p[b];
+        const word_t q = __shfl_xor_sync(0xffffffffu, a, off);
+        p[b] = a ^ q ^ carry;
+        carry = (a & q) | (carry & (a ^ q));
+      }
+    }
+  }
+  __device__ __forceinline__ unsigned count_of(int j) const {
+    unsigned v = 0;
+#pragma unroll
+    for (int b = 0; b < B; ++b) v |= (unsigned)((p[b] >> j) & 1ULL) << b;
+    return v;
+  }
+};
+
+// Adds q0 + 2*q1 (two bit-planes) into a 4-plane counter whose values stay
+// below 16 (the caller flushes it often enough).
+__device__ __forceinline__ void add2_small(VCount<4>& a, word_t q0, word_t q1) {
+  word_t t0 = a.p[0] & q0;
+  a.p[0] ^= q0;
+  word_t s1 = a.p[1] ^ t0 ^ q1;
+  word_t c1 = (a.p[1] & t0) | (q1 & (a.p[1] ^ t0));
+  a.p[1] = s1;
+  word_t t2 = a.p[2] & c1;
+  a.p[2] ^= c1;
+  a.p[3] ^= t2;
+}
+
+// big += small (small has 4 planes, big B >= 4).
+template <int B>
+__device__ __forceinline__ void add_small(VCount<B>& big, const VCount<4>& sm) {
+  word_t carry = 0;
+#pragma unroll
+  for (int b = 0; b < B; ++b) {
+    word_t q = (b < 4) ? sm.p[b] : 0;
+    word_t a = big.p[b];
+    big.p[b] = a ^ q ^ carry;
+    carry = (a & q) | (carry & (a ^ q));
+  }
 }
 
 }  // namespace sa

@@ -6,7 +6,7 @@
 #include <cstdint>
 #include <string>
 
-#include "sa_device.cuh"
+#include "sa_types.hpp"
 
 namespace sa {
 

@@ -126,50 +126,6 @@ __global__ void __launch_bounds__(128) k_halfsweep_3d(word_t* __restrict__ s,
   }
 }
 
-// Bit-sliced vertical counter: plane b holds bit b of 64 per-replica counts.
-template <int B>
-struct VCount {
-  word_t p[B];
-  __device__ __forceinline__ void clear() {
-#pragma unroll
-    for (int b = 0; b < B; ++b) p[b] = 0;
-  }
-  __device__ __forceinline__ void add(word_t m) {
-    word_t carry = m;
-#pragma unroll
-    for (int b = 0; b < B; ++b) {
-      word_t t = p[b] & carry;
-      p[b] ^= carry;
-      carry = t;
-    }
-  }
-  __device__ __forceinline__ void add_counter(const VCount& o) {
-    word_t carry = 0;
-#pragma unroll
-    for (int b = 0; b < B; ++b) {
-      word_t a = p[b], q = o.p[b];
-      p[b] = a ^ q ^ carry;
-      carry = (a & q) | (carry & (a ^ q));
-    }
-  }
-  // Sum over the lanes of a warp (result valid in every lane).
-  __device__ __forceinline__ void warp_sum() {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      VCount o;
-#pragma unroll
-      for (int b = 0; b < B; ++b) o.p[b] = __shfl_xor_sync(0xffffffffu, p[b], off);
-      add_counter(o);
-    }
-  }
-  __device__ __forceinline__ unsigned count_of(int j) const {
-    unsigned v = 0;
-#pragma unroll
-    for (int b = 0; b < B; ++b) v |= (unsigned)((p[b] >> j) & 1ULL) << b;
-    return v;
-  }
-};
-
 constexpr int kMeasureThreads = 256;
 constexpr int kMeasureMaxSitesPerThread = 512;  // 3 bonds each: per-warp sum < 2^16
 

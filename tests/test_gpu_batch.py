@@ -1,0 +1,134 @@
+"""GPU parity of the batched persistent engine against the oracle.
+
+Each batched instance must reproduce, bit for bit, the reference's
+parallel_tempering<> (src/parallel_tempering.hpp:81-115) over systems built as
+its driver builds them (src/main_gpu.cu:262-276) -- restated by the oracle in
+PHILOX mode: every exchange pair and mask, every spin word of every slot, the
+acceptance counters; anneal instances reproduce annealing<> with a linear
+schedule (running maximum of -H per replica, src/annealing.hpp:67-100).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_pt(lat, L, T, seed_J, seed, nsweeps, interval=1):
+    systems = [O.OracleSystem(lat, L, mode=O.MODE_PHILOX) for _ in T]
+    for s in systems:
+        s.set_seed(seed_J)
+        s.init_J()
+        s.set_seed(seed)
+        s.init_rand()
+    pt = O.OraclePT(systems, T, interval)
+    steps = [pt.step(0) for _ in range(nsweeps // interval)]
+    return systems, pt, steps
+
+
+def check_instance(b, i, lat, L, T, seed_J, seed, nsweeps, interval=1):
+    systems, pt, steps = oracle_pt(lat, L, T, seed_J, seed, nsweeps, interval)
+    pairs, masks = b.exchanges(i)
+    assert pairs.tolist() == [p for p, _, _ in steps]
+    assert [int(m) for m in masks] == [m for _, m, _ in steps]
+    for slot, s in enumerate(systems):
+        assert np.array_equal(b.spins(i, slot), s.spins()), (i, slot)
+        assert np.array_equal(b.measure(i, slot), s.measure()[0]), (i, slot)
+    acc, att = b.acceptance(i)
+    ref = pt.acceptance()
+    assert np.allclose(acc / np.maximum(att, 1) / 64.0, ref, rtol=0, atol=1e-12)
+    jo = systems[0].J()
+    for a, c in zip(b.J(i), jo):
+        assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("nslots", [2, 3, 5, 8, 16, 32])
+def test_pt_batch_all_lane_classes(sab, nslots):
+    from simulated_annealing_b200.batch import Batch
+    T = list(np.geomspace(0.4, 2.1, nslots))
+    b = Batch()
+    lad = b.add_ladder(T)
+    specs = [(O.LAT_2D, 6, 11), (O.LAT_2D_OPEN_X, 8, 12), (O.LAT_3D, 4, 13), (O.LAT_3D, 6, 14)]
+    for lat, L, s in specs:
+        b.add_instance(lat, L, ladder=lad, seed_J=s, seed=s + 50)
+    b.finalize()
+    b.record_exchanges(64)
+    b.run(5)
+    b.run(4)  # continuation across launches
+    b.sync()
+    for i, (lat, L, s) in enumerate(specs):
+        check_instance(b, i, lat, L, T, s, s + 50, 9)
+
+
+def test_c4_shapes_subset(sab):
+    """One instance of each C4 shape, 16 geometric slots, 12 sweeps."""
+    from simulated_annealing_b200.batch import Batch
+    b = Batch()
+    l2 = b.add_ladder(np.geomspace(0.3, 1.6, 16))
+    l3 = b.add_ladder(np.geomspace(0.5, 2.0, 16))
+    specs = [(O.LAT_2D, L, 1000 + k) for k, L in enumerate([16, 24, 32, 48, 64])]
+    specs += [(O.LAT_3D, L, 1005 + k) for k, L in enumerate([8, 12, 16, 20, 24])]
+    for lat, L, s in specs:
+        b.add_instance(lat, L, ladder=(l3 if lat == O.LAT_3D else l2), seed_J=s, seed=s)
+    b.finalize()
+    b.record_exchanges(32)
+    b.run(12)
+    b.sync()
+    for i, (lat, L, s) in enumerate(specs):
+        T = np.geomspace(0.5, 2.0, 16) if lat == O.LAT_3D else np.geomspace(0.3, 1.6, 16)
+        check_instance(b, i, lat, L, list(T), s, s, 12)
+
+
+def test_exchange_interval(sab):
+    from simulated_annealing_b200.batch import Batch
+    T = [0.5, 0.8, 1.3]
+    b = Batch()
+    lad = b.add_ladder(T)
+    b.add_instance(O.LAT_3D, 4, ladder=lad, seed_J=3, seed=4)
+    b.finalize()
+    b.set_exchange_interval(3)
+    b.record_exchanges(16)
+    b.run(9)
+    b.sync()
+    check_instance(b, 0, O.LAT_3D, 4, T, 3, 4, 9, interval=3)
+
+
+def test_anneal_instances_linear_schedule(sab):
+    from simulated_annealing_b200.batch import Batch
+    nsteps, per = 6, 5
+    T0, T1 = 3.0, 0.2
+    Ts = [T0 + (T1 - T0) * k / (nsteps - 1) for k in range(nsteps)]
+    b = Batch()
+    sch = b.add_schedule(Ts, per)
+    specs = [(O.LAT_2D, 8, 21), (O.LAT_3D, 6, 22), (O.LAT_2D_OPEN_X, 10, 23)]
+    for lat, L, s in specs:
+        b.add_instance(lat, L, schedule=sch, seed_J=s, seed=s + 1)
+    b.finalize()
+    b.run(7)
+    b.run(100)  # stops at the end of the schedule
+    b.sync()
+    for i, (lat, L, s) in enumerate(specs):
+        o = O.OracleSystem(lat, L, mode=O.MODE_PHILOX)
+        o.set_seed(s)
+        o.init_J()
+        o.set_seed(s + 1)
+        o.init_rand()
+        mn, _ = o.anneal(T0, 1, T1, nsteps, per, 1)
+        E, done = b.anneal_result(i)
+        assert done == nsteps * per
+        assert np.array_equal(E.astype(np.float32), mn)
+        assert np.array_equal(b.spins(i, 0), o.spins())
+
+
+def test_bad_instances_rejected(sab):
+    from simulated_annealing_b200._lib import SAError
+    from simulated_annealing_b200.batch import Batch
+    b = Batch()
+    lad = b.add_ladder([1.0, 2.0])
+    with pytest.raises(SAError):
+        b.add_instance(O.LAT_2D, 7, ladder=lad, seed_J=1, seed=1)
+    with pytest.raises(SAError):
+        b.add_instance(O.LAT_3D, 128, ladder=lad, seed_J=1, seed=1)
+    with pytest.raises(SAError):
+        b.add_ladder(np.linspace(1, 2, 33))
