@@ -233,7 +233,7 @@ def run_ours(args):
     S = args.sweeps_per_step
     site_slots = b.site_slots()
     attempts_step = site_slots * 64 * S
-    n_classes = 1  # every instance has 16 slots: one persistent launch per step
+    n_classes = b.launches_per_run()  # one launch per (lanes-per-site, cluster size) group
 
     def barrier():
         torch.cuda.synchronize()

@@ -51,6 +51,13 @@ int sa_batch_add_instance(sa_batch_t b, int lattice, int L, int ladder_id, int s
  * the device and uploads the tables. No instance may be added afterwards. */
 int sa_batch_finalize(sa_batch_t b);
 
+/* Kernel choice, before finalize: 0 (default) keeps every instance whose
+ * spins fit in the shared memory of a cluster of <= 16 CTAs resident there for
+ * a whole launch and runs the rest in the global-memory kernel; 1 runs every
+ * instance in the global-memory kernel. */
+int sa_batch_set_kernel(sa_batch_t b, int kernel);
+/* Kernel launches one sa_batch_run issues (one per launch group). */
+int sa_batch_launches_per_run(sa_batch_t b, int* n);
 /* Sweeps between exchange attempts (the PT template's `steps`; default 1). */
 int sa_batch_set_exchange_interval(sa_batch_t b, int sweeps_per_exchange);
 /* Anneal instances: measure every `stride` sweeps (0 = never; default 1) and

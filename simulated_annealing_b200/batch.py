@@ -33,6 +33,8 @@ for _name, _res, _args in [
     ("sa_batch_finalize", _c.c_int, [_vp]),
     ("sa_batch_set_exchange_interval", _c.c_int, [_vp, _c.c_int]),
     ("sa_batch_set_measure_stride", _c.c_int, [_vp, _c.c_int]),
+    ("sa_batch_set_kernel", _c.c_int, [_vp, _c.c_int]),
+    ("sa_batch_launches_per_run", _c.c_int, [_vp, _ip]),
     ("sa_batch_record_exchanges", _c.c_int, [_vp, _c.c_long]),
     ("sa_batch_run", _c.c_int, [_vp, _c.c_long]),
     ("sa_batch_sync", _c.c_int, [_vp]),
@@ -61,12 +63,20 @@ def _p(a, ct):
     return a.ctypes.data_as(_c.POINTER(ct))
 
 
+KERNEL_AUTO, KERNEL_GLOBAL = 0, 1
+
+
 class Batch:
-    def __init__(self):
+    """kernel: KERNEL_AUTO keeps instances resident in cluster shared memory
+    where they fit; KERNEL_GLOBAL streams every instance from global memory."""
+
+    def __init__(self, kernel: int = KERNEL_AUTO):
         self._lib = _lib.load()
         h = _vp()
         check(self._lib.sa_batch_create(_c.byref(h)))
         self._h = h
+        if kernel != KERNEL_AUTO:
+            check(self._lib.sa_batch_set_kernel(self._h, int(kernel)))
         self.instances = []  # (lattice, L, nslots)
         self._ladders = []
         self._final = False
@@ -116,6 +126,11 @@ class Batch:
 
     def set_stream(self, stream_ptr: int) -> None:
         check(self._lib.sa_batch_set_stream(self._h, _vp(stream_ptr)))
+
+    def launches_per_run(self) -> int:
+        n = _c.c_int()
+        check(self._lib.sa_batch_launches_per_run(self._h, _c.byref(n)))
+        return n.value
 
     def site_slots(self) -> int:
         n = _c.c_longlong()

@@ -29,6 +29,7 @@
 #include "sa_batch.hpp"
 #include "sa_device.cuh"
 #include "sa_host.hpp"
+#include "sa_resident.cuh"
 
 namespace sa {
 
@@ -353,6 +354,159 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchParams p) {
 }
 
 // ---------------------------------------------------------------------------
+// Shared-memory-resident kernel: one cluster of C CTAs per instance.
+// ---------------------------------------------------------------------------
+template <int P>
+__global__ void __launch_bounds__(kResThreads, 1) k_resident(BatchParams p) {
+  extern __shared__ __align__(16) word_t s_spins[];
+  __shared__ unsigned s_cnt[2][64];   // this CTA's partial counts
+  __shared__ unsigned s_tot[2][64];   // cluster totals
+  __shared__ unsigned s_mask[2];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int C = (int)cluster.num_blocks();
+  const int q = (int)cluster.block_rank();
+  const int id = p.order[blockIdx.x / C];
+  const InstDesc d = p.inst[id];
+  InstState* st = p.state + id;
+  const uint64_t draw0 = st->draw;
+  const int64_t sweeps0 = st->sweeps, xsteps0 = st->xsteps;
+  int64_t n = p.nsweeps;
+  if (d.sweep_limit >= 0) n = min(n, d.sweep_limit - sweeps0);
+  if (n <= 0) return;  // the whole cluster sees the same n
+
+  ResCtx x;
+  x.L = d.L;
+  x.hL = d.L >> 1;
+  x.ns = d.nslots;
+  x.zc = (d.lattice == SA_LATTICE_3D) ? d.L : 1;
+  x.ny = d.L / C;
+  x.y0 = q * x.ny;
+  x.rowW = x.hL * x.ns;
+  x.half = (int)d.half;
+  x.seed = d.seed;
+  x.magic = (uint32_t)(0xFFFFFFFFu / (uint32_t)x.hL) + 1u;
+  x.sm = s_spins;
+  x.smN = cluster.map_shared_rank(s_spins, (unsigned)((q + C - 1) % C));
+  x.smS = cluster.map_shared_rank(s_spins, (unsigned)((q + 1) % C));
+  x.J = p.J + d.J_off;
+  const bool d3 = d.lattice == SA_LATTICE_3D, open = d.lattice == SA_LATTICE_2D_OPEN_X;
+
+  // global [colour][row = y + L*z][k][slot] -> local [colour][z][y_local][k][slot]
+  word_t* gS = p.spins + d.spin_off;
+  const int blk = x.ny * x.rowW;
+  for (int cz = 0; cz < 2 * x.zc; ++cz) {
+    const int c = cz / x.zc, z = cz - c * x.zc;
+    const word_t* src = gS + ((long)c * d.half + (long)(z * x.L + x.y0) * x.hL) * x.ns;
+    word_t* dst = s_spins + (long)cz * blk;
+    for (int i = threadIdx.x; i < blk; i += blockDim.x) dst[i] = src[i];
+  }
+  cluster.sync();
+
+  const int lane = threadIdx.x & 31;
+  const int slot = lane % P;
+  uint32_t th[8], tb[8];
+  int64_t step = -1;
+  if (d.sched < 0) {
+    const BThr* t = p.thr + d.thr_off + (slot < d.nslots ? slot : 0);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { th[k] = t->dn[k]; tb[k] = t->bdn[k]; }
+  }
+  uint64_t draw = draw0;
+  int64_t sweeps = sweeps0, xsteps = xsteps0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (d.sched >= 0) {
+      int64_t s = sweeps / d.sweeps_per_step;
+      if (s > d.thr_count - 1) s = d.thr_count - 1;
+      if (s != step) {
+        step = s;
+        const BThr* t = p.thr + d.thr_off + s;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) { th[k] = t->dn[k]; tb[k] = t->bdn[k]; }
+      }
+    }
+    for (int c = 0; c < 2; ++c) {
+      if (d3) rhalf_3d<P>(x, c, draw + c, th);
+      else if (open) rhalf_2d<P, true>(x, c, draw + c, th, tb);
+      else rhalf_2d<P, false>(x, c, draw + c, th, tb);
+      cluster.sync();
+    }
+    draw += 2;
+    const int64_t in_step = (d.sched >= 0) ? sweeps % d.sweeps_per_step : 0;
+    sweeps += 1;
+    const bool xchg = d.ladder >= 0 && d.nslots > 1 && sweeps % p.xinterval == 0;
+    const bool meas = d.sched >= 0 && p.mstride > 0 && in_step % p.mstride == 0;
+    if (xchg || meas) {
+      Decision dc = {0, 0, 0, 0};
+      int a = 0, nsl = 1;
+      if (xchg) {
+        dc = p.dec[d.dec_off + xsteps];
+        a = dc.pair;
+        nsl = 2;
+      }
+      rmeasure(x, d3, open, a, nsl, s_cnt);
+      cluster.sync();
+      if (threadIdx.x < 128) {
+        unsigned v = 0;
+        for (int r = 0; r < C; ++r) v += cluster.map_shared_rank(&s_cnt[0][0], (unsigned)r)[threadIdx.x];
+        (&s_tot[0][0])[threadIdx.x] = v;
+      }
+      __syncthreads();
+      if (xchg) {
+        if (threadIdx.x < 64) {
+          const int j = threadIdx.x;
+          const int64_t dE = 2 * ((int64_t)s_tot[1][j] - (int64_t)s_tot[0][j]);
+          const bool acc = dE >= dc.lo && dE <= dc.hi;
+          const unsigned bal = __ballot_sync(0xffffffffu, acc);
+          if (lane == 0) s_mask[threadIdx.x >> 5] = bal;
+        }
+        __syncthreads();
+        const word_t mask = (word_t)s_mask[0] | ((word_t)s_mask[1] << 32);
+        if (mask) {
+          const int nloc = 2 * x.zc * x.ny * x.hL;
+          for (int t = threadIdx.x; t < nloc; t += blockDim.x) {
+            word_t* w = s_spins + (long)t * x.ns + a;
+            const word_t x0 = w[0], x1 = w[1];
+            const word_t dd = (x0 ^ x1) & mask;
+            w[0] = x0 ^ dd;
+            w[1] = x1 ^ dd;
+          }
+        }
+        if (q == 0 && threadIdx.x == 0) {
+          p.acc[d.pair_off + a] += __popcll(mask);
+          p.att[d.pair_off + a] += 1;
+          if (p.rec_pair && xsteps < p.rec_cap) {
+            p.rec_pair[(long)id * p.rec_cap + xsteps] = a;
+            p.rec_mask[(long)id * p.rec_cap + xsteps] = mask;
+          }
+        }
+        xsteps += 1;
+      } else if (q == 0 && threadIdx.x < 64) {
+        const int j = threadIdx.x;
+        const int64_t e = 2 * (int64_t)s_tot[0][j] - d.nbonds;
+        const int64_t m0 = st->measured;
+        st->elast[j] = e;
+        st->emax[j] = (m0 == 0) ? e : max(st->emax[j], e);
+      }
+      cluster.sync();
+      if (meas && q == 0 && threadIdx.x == 0) st->measured += 1;
+    }
+  }
+  // local -> global
+  for (int cz = 0; cz < 2 * x.zc; ++cz) {
+    const int c = cz / x.zc, z = cz - c * x.zc;
+    word_t* dst = gS + ((long)c * d.half + (long)(z * x.L + x.y0) * x.hL) * x.ns;
+    const word_t* src = s_spins + (long)cz * blk;
+    for (int i = threadIdx.x; i < blk; i += blockDim.x) dst[i] = src[i];
+  }
+  if (q == 0 && threadIdx.x == 0) {
+    st->draw = draw;
+    st->sweeps = sweeps;
+    st->xsteps = xsteps;
+  }
+  cluster.sync();  // no CTA leaves while a peer may still read its shared memory
+}
+
+// ---------------------------------------------------------------------------
 // Set-up kernels: couplings from seed_J (draws 0..2*dim-1, src/random.cu:25-35)
 // and spins (engine init, epoch 0) copied into every slot.
 // ---------------------------------------------------------------------------
@@ -471,21 +625,37 @@ struct sa_batch {
   int64_t h2d_bytes_last = 0;  // host->device bytes of the last sa_batch_run
   int64_t* d_Eall = nullptr;   // all-slot energies
   int64_t e_count = 0;         // sum of nslots*64
-  // work classes by lanes-per-site P = 1,2,4,8,16,32: a contiguous range of
-  // the work order each, one persistent launch per non-empty class
-  int cls_begin[6] = {0, 0, 0, 0, 0, 0};
-  int cls_count[6] = {0, 0, 0, 0, 0, 0};
-  int cls_grid[6] = {0, 0, 0, 0, 0, 0};
+  bool force_global = false;   // run every instance in the global-memory kernel
+  // Launch groups: a contiguous range of the work order sharing the kernel
+  // (resident or global), the lanes-per-site P and the cluster size C.
+  struct Group {
+    bool resident;
+    int P, C, begin, count, grid;
+    size_t smem;
+  };
+  std::vector<Group> groups;
+  std::vector<int> cluster_of;  // per instance: C (0 = global-memory kernel)
 };
 
-static int p_class(int P) {
-  int c = 0;
-  while ((1 << c) < P) ++c;
-  return c;
+// Shared-memory budget of one CTA of the resident kernel (the rest of the
+// 227 KB opt-in limit holds its static arrays).
+constexpr size_t kResSmemBudget = 224 * 1024;
+
+// Smallest cluster size C dividing L whose per-CTA share of the instance's
+// spins fits the budget; 0 if none does (the instance then runs in the
+// global-memory kernel).
+static int choose_cluster(const InstDesc& d) {
+  static const int cands[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
+  const size_t bytes = (size_t)d.N * d.nslots * sizeof(word_t);
+  for (int C : cands) {
+    if (C > d.L || d.L % C) continue;
+    if (bytes / C <= kResSmemBudget) return C;
+  }
+  return 0;
 }
 
 template <int P>
-static void launch_class(sa_batch* b, int cls, long nsweeps);
+static int launch_group(sa_batch* b, const sa_batch::Group& g, int gi, long nsweeps);
 
 static BThr to_bthr(int lattice, double T) {
   Thresholds t;
@@ -584,13 +754,68 @@ static int ensure_decisions(sa_batch* b, const std::vector<int64_t>& need) {
 }
 
 template <int P>
-static void launch_class(sa_batch* b, int cls, long nsweeps) {
+static int launch_group(sa_batch* b, const sa_batch::Group& g, int gi, long nsweeps) {
   BatchParams p;
   batch_params(b, nsweeps, &p);
-  p.order = b->d_order + b->cls_begin[cls];
-  p.ninst = b->cls_count[cls];
-  p.work = b->d_work + cls;
-  k_batch<P><<<b->cls_grid[cls], kBatchThreads, 0, b->stream>>>(p);
+  p.order = b->d_order + g.begin;
+  p.ninst = g.count;
+  p.work = b->d_work + gi;
+  if (!g.resident) {
+    k_batch<P><<<g.grid, kBatchThreads, 0, b->stream>>>(p);
+    SA_CUDA_TRY(cudaGetLastError());
+    return SA_OK;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(g.count * g.C), 1, 1);
+  cfg.blockDim = dim3(kResThreads, 1, 1);
+  cfg.dynamicSmemBytes = g.smem;
+  cfg.stream = b->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)g.C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  SA_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_resident<P>, p));
+  return SA_OK;
+}
+
+template <int P>
+static int prepare_resident(const sa_batch::Group& g, int* max_clusters) {
+  SA_CUDA_TRY(cudaFuncSetAttribute(k_resident<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
+  if (g.C > 8) SA_CUDA_TRY(cudaFuncSetAttribute(k_resident<P>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)g.C, 1, 1);
+  cfg.blockDim = dim3(kResThreads, 1, 1);
+  cfg.dynamicSmemBytes = g.smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)g.C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  SA_CUDA_TRY(cudaOccupancyMaxActiveClusters(max_clusters, k_resident<P>, &cfg));
+  return SA_OK;
+}
+
+template <int P>
+static int group_dispatch(sa_batch* b, const sa_batch::Group& g, int gi, long nsweeps, int prepare,
+                          int* max_clusters) {
+  if (prepare) return g.resident ? prepare_resident<P>(g, max_clusters) : SA_OK;
+  return launch_group<P>(b, g, gi, nsweeps);
+}
+
+static int dispatch(sa_batch* b, const sa_batch::Group& g, int gi, long nsweeps, int prepare, int* mc) {
+  switch (g.P) {
+    case 1: return group_dispatch<1>(b, g, gi, nsweeps, prepare, mc);
+    case 2: return group_dispatch<2>(b, g, gi, nsweeps, prepare, mc);
+    case 4: return group_dispatch<4>(b, g, gi, nsweeps, prepare, mc);
+    case 8: return group_dispatch<8>(b, g, gi, nsweeps, prepare, mc);
+    case 16: return group_dispatch<16>(b, g, gi, nsweeps, prepare, mc);
+    default: return group_dispatch<32>(b, g, gi, nsweeps, prepare, mc);
+  }
 }
 
 extern "C" {
@@ -736,24 +961,37 @@ int sa_batch_finalize(sa_batch_t b) {
     d.thr_off = it->second;
   }
   b->npairs = pair_off;
-  // work order: grouped by P class, most expensive first inside a class
+  // work order: grouped by (kernel, P, C), most expensive first inside a group
+  b->cluster_of.resize(b->inst.size());
+  for (size_t i = 0; i < b->inst.size(); ++i) b->cluster_of[i] = b->force_global ? 0 : choose_cluster(b->inst[i]);
   std::vector<int32_t> order(b->inst.size());
   for (size_t i = 0; i < order.size(); ++i) order[i] = (int32_t)i;
   std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
     const InstDesc &dx = b->inst[x], &dy = b->inst[y];
+    const int cx = b->cluster_of[x], cy = b->cluster_of[y];
+    if ((cx == 0) != (cy == 0)) return cx != 0;
     if (dx.P != dy.P) return dx.P < dy.P;
+    if (cx != cy) return cx > cy;
     return dx.N * dx.nslots > dy.N * dy.nslots;
   });
+  b->groups.clear();
   for (size_t i = 0; i < order.size(); ++i) {
-    const int c = p_class(b->inst[order[i]].P);
-    if (b->cls_count[c] == 0) b->cls_begin[c] = (int)i;
-    b->cls_count[c] += 1;
+    const InstDesc& d = b->inst[order[i]];
+    const int C = b->cluster_of[order[i]];
+    const size_t smem = C ? (size_t)d.N * d.nslots * sizeof(word_t) / C : 0;
+    if (b->groups.empty() || b->groups.back().resident != (C != 0) || b->groups.back().P != d.P ||
+        b->groups.back().C != C) {
+      b->groups.push_back({C != 0, d.P, C, (int)i, 0, 0, 0});
+    }
+    sa_batch::Group& g = b->groups.back();
+    g.count += 1;
+    g.smem = std::max(g.smem, smem);
   }
   const size_t ni = b->inst.size();
   SA_CUDA_TRY(cudaMalloc(&b->d_inst, ni * sizeof(InstDesc)));
   SA_CUDA_TRY(cudaMalloc(&b->d_state, ni * sizeof(InstState)));
   SA_CUDA_TRY(cudaMalloc(&b->d_order, ni * sizeof(int32_t)));
-  SA_CUDA_TRY(cudaMalloc(&b->d_work, 6 * sizeof(int32_t)));
+  SA_CUDA_TRY(cudaMalloc(&b->d_work, std::max<size_t>(b->groups.size(), 1) * sizeof(int32_t)));
   SA_CUDA_TRY(cudaMalloc(&b->d_spins, std::max<int64_t>(spin_off, 1) * sizeof(word_t)));
   SA_CUDA_TRY(cudaMalloc(&b->d_J, std::max<int64_t>(J_off, 1) * sizeof(word_t)));
   SA_CUDA_TRY(cudaMalloc(&b->d_thr, std::max<size_t>(thr.size(), 1) * sizeof(BThr)));
@@ -782,13 +1020,17 @@ int sa_batch_finalize(sa_batch_t b) {
   b->h_xsteps.assign(ni, 0);
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-  const void* kernels[6] = {(const void*)k_batch<1>, (const void*)k_batch<2>, (const void*)k_batch<4>,
-                            (const void*)k_batch<8>, (const void*)k_batch<16>, (const void*)k_batch<32>};
-  for (int c = 0; c < 6; ++c) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernels[c], kBatchThreads, 0);
-    if (per_sm < 1) per_sm = 1;
-    b->cls_grid[c] = (int)std::min<int64_t>((int64_t)sms * per_sm, (int64_t)b->cls_count[c]);
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    sa_batch::Group& g = b->groups[gi];
+    if (g.resident) {
+      int mc = 0;
+      int st = dispatch(b, g, (int)gi, 0, 1, &mc);
+      if (st) return st;
+      if (mc < 1) return fail(SA_ERR_UNSUPPORTED, "a resident cluster cannot be scheduled on this device");
+      g.grid = mc;
+    } else {
+      g.grid = (int)std::min<int64_t>((int64_t)sms, (int64_t)g.count);  // one 512-thread CTA per SM
+    }
   }
   b->finalized = true;
   // the ladders' first exchanges
@@ -799,6 +1041,19 @@ int sa_batch_finalize(sa_batch_t b) {
 int sa_batch_set_exchange_interval(sa_batch_t b, int k) {
   if (!b || k < 1) return fail(SA_ERR_INVALID, "interval must be >= 1");
   b->xinterval = k;
+  return SA_OK;
+}
+
+int sa_batch_set_kernel(sa_batch_t b, int kernel) {
+  if (!b || kernel < 0 || kernel > 1) return fail(SA_ERR_INVALID, "kernel must be 0 (auto) or 1 (global)");
+  if (b->finalized) return fail(SA_ERR_INVALID, "choose the kernel before finalize");
+  b->force_global = (kernel == 1);
+  return SA_OK;
+}
+
+int sa_batch_launches_per_run(sa_batch_t b, int* n) {
+  if (!b || !n) return fail(SA_ERR_INVALID, "null argument");
+  *n = (int)b->groups.size();
   return SA_OK;
 }
 
@@ -849,13 +1104,11 @@ int sa_batch_run(sa_batch_t b, long nsweeps) {
   b->h2d_bytes_last = 0;
   int st = ensure_decisions(b, need);
   if (st) return st;
-  SA_CUDA_TRY(cudaMemsetAsync(b->d_work, 0, 6 * sizeof(int32_t), b->stream));
-  if (b->cls_count[0]) launch_class<1>(b, 0, nsweeps);
-  if (b->cls_count[1]) launch_class<2>(b, 1, nsweeps);
-  if (b->cls_count[2]) launch_class<4>(b, 2, nsweeps);
-  if (b->cls_count[3]) launch_class<8>(b, 3, nsweeps);
-  if (b->cls_count[4]) launch_class<16>(b, 4, nsweeps);
-  if (b->cls_count[5]) launch_class<32>(b, 5, nsweeps);
+  SA_CUDA_TRY(cudaMemsetAsync(b->d_work, 0, b->groups.size() * sizeof(int32_t), b->stream));
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    st = dispatch(b, b->groups[gi], (int)gi, nsweeps, 0, nullptr);
+    if (st) return st;
+  }
   SA_CUDA_TRY(cudaGetLastError());
   return SA_OK;
 }

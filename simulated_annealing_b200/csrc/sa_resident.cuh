@@ -1,0 +1,252 @@
+// sa_resident.cuh -- the shared-memory-resident batched kernel.
+//
+// One instance (all its slots) is held in the shared memory of a thread-block
+// cluster of C CTAs for a whole launch: CTA q owns the y-rows
+// [q*L/C, (q+1)*L/C) of every z-plane and both colours, layout
+//   [colour][z][y_local][k][slot]            (k = x/2, slot innermost)
+// and reads the two halo rows it needs (y0-1, y0+ny) from the neighbouring
+// CTAs' shared memory over DSMEM. Couplings stay in global memory (L2) and
+// are shared by the slots of a site. Between half-sweeps the cluster
+// synchronises; the replica exchange sums per-CTA energy partials over DSMEM,
+// so every CTA reaches the same decision and swaps its own rows.
+//
+// Spins go HBM -> shared memory once at the start of a launch and back once at
+// the end, so a launch of S sweeps moves 2*8 bytes per site and slot through
+// HBM instead of ~24*S.
+#pragma once
+#include <cooperative_groups.h>
+
+#include "sa_batch.hpp"
+#include "sa_device.cuh"
+
+namespace sa {
+
+namespace cg = cooperative_groups;
+
+constexpr int kResThreads = 512;
+
+struct ResCtx {
+  word_t* sm;           // this CTA's rows
+  const word_t* smN;    // CTA owning row y0-1 (generic pointer; self when C == 1)
+  const word_t* smS;    // CTA owning row y0+ny
+  const word_t* J;      // instance couplings [axis][colour][row][k] (global)
+  uint64_t seed;
+  int L, hL, ny, y0, ns, zc;  // zc: z-planes (L in 3D, 1 in 2D)
+  int half;                   // sites per colour of the instance (global J stride)
+  int rowW;                   // words per local row: hL*ns
+  uint32_t magic;             // floor(2^32/hL)+1, for division by hL
+};
+
+// t / hL for t < 2^20, hL <= 2^11, with one correction step.
+__device__ __forceinline__ int div_hl(int t, const ResCtx& x) {
+  int q = (int)__umulhi((unsigned)t, x.magic);
+  if ((q + 1) * x.hL <= t) ++q;
+  if (q * x.hL > t) --q;
+  return q;
+}
+
+// local word offset of (colour, z, y_local) row start
+__device__ __forceinline__ int lrow(const ResCtx& x, int c, int z, int yl) {
+  return ((c * x.zc + z) * x.ny + yl) * x.rowW;
+}
+
+template <int P, bool OPEN_X>
+__device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, const uint32_t* th,
+                                         const uint32_t* tb) {
+  constexpr int SPS = 32 / P;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int slot = lane % P;
+  const bool slot_ok = slot < x.ns;
+  const int tot = x.ny * x.hL;
+  const int L = x.L, hL = x.hL, ns = x.ns;
+  const int oc = 1 - c;
+  const word_t* Jxc = x.J + (long)(0 + c) * x.half;
+  const word_t* Jxo = x.J + (long)(1 - c) * x.half;
+  const word_t* Jyc = x.J + (long)(2 + c) * x.half;
+  const word_t* Jyo = x.J + (long)(3 - c) * x.half;
+  for (int base = warp * 32; base < tot; base += nwarps * 32) {
+    const int my = base + lane;
+    uint32_t um = 0;
+    if (my < tot) {
+      const int yl = div_hl(my, x);
+      const int k = my - yl * hL, y = x.y0 + yl;
+      const int xx = 2 * k + ((c + y) & 1);
+      um = philox_draw(x.seed, (unsigned long long)(xx + L * y), draw);
+    }
+#pragma unroll 1
+    for (int sub = 0; sub < P; ++sub) {
+      const int sl = sub * SPS + lane / P;
+      const uint32_t u = __shfl_sync(0xffffffffu, um, sl);
+      const int t = base + sl;
+      if (t < tot && slot_ok) {
+        const int yl = div_hl(t, x);
+        const int k = t - yl * hL, y = x.y0 + yl;
+        const int par = (c + y) & 1, xx = 2 * k + par;
+        int kw, ke;
+        x_neighbours(k, par, hL, kw, ke);
+        const int own = lrow(x, c, 0, yl) + k * ns + slot;
+        const int orow = lrow(x, oc, 0, yl);
+        const word_t* pn = (yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow(x, oc, 0, x.ny - 1);
+        const word_t* ps = (yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow(x, oc, 0, 0);
+        const int ys = (y == L - 1) ? 0 : y + 1;
+        const word_t si = x.sm[own];
+        word_t mw = __ldg(Jxc + y * hL + k) ^ x.sm[orow + kw * ns + slot] ^ si;
+        word_t me = __ldg(Jxo + y * hL + ke) ^ x.sm[orow + ke * ns + slot] ^ si;
+        const word_t mn = __ldg(Jyc + y * hL + k) ^ pn[k * ns + slot] ^ si;
+        const word_t ms = __ldg(Jyo + ys * hL + k) ^ ps[k * ns + slot] ^ si;
+        bool border = false;
+        if (OPEN_X) {
+          if (xx == 0) { mw = ~0ULL; border = true; }
+          if (xx == L - 1) { me = ~0ULL; border = true; }
+        }
+        word_t c0, c1, c2;
+        count4(mw, me, mn, ms, c0, c1, c2);
+        const uint32_t tt = (OPEN_X && border) ? prefix_count<4>(u, tb) : prefix_count<4>(u, th);
+        x.sm[own] = si ^ ~ge_scalar(c0, c1, c2, tt);
+      }
+    }
+  }
+}
+
+template <int P>
+__device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, const uint32_t* th) {
+  constexpr int SPS = 32 / P;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int slot = lane % P, cl = lane / P;
+  const bool slot_ok = slot < x.ns;
+  const int L = x.L, hL = x.hL, ns = x.ns;
+  const int cols = x.ny * hL;
+  const int oc = 1 - c;
+  const int zs = x.ny * x.rowW;   // local z stride
+  const int zg = L * hL;          // global z stride of the coupling arrays
+  const word_t* Jxc = x.J + (long)(0 + c) * x.half;
+  const word_t* Jxo = x.J + (long)(1 - c) * x.half;
+  const word_t* Jyc = x.J + (long)(2 + c) * x.half;
+  const word_t* Jyo = x.J + (long)(3 - c) * x.half;
+  const word_t* Jzc = x.J + (long)(4 + c) * x.half;
+  for (int cb = warp * SPS; cb < cols; cb += nwarps * SPS) {
+    const int col = cb + cl;
+    const bool col_ok = col < cols;
+    const bool valid = col_ok && slot_ok;
+    const int yl = col_ok ? div_hl(col, x) : 0;
+    const int k = col_ok ? col - yl * hL : 0;
+    const int y = x.y0 + yl;
+    const int par = (c + y) & 1, xx = 2 * k + par;
+    int kw, ke;
+    x_neighbours(k, par, hL, kw, ke);
+    const int ys = (y == L - 1) ? 0 : y + 1;
+    // z = 0 offsets; every z step adds zs (shared) or zg (couplings)
+    int own = lrow(x, c, 0, yl) + k * ns + slot;
+    int ow = lrow(x, oc, 0, yl) + kw * ns + slot;
+    int oe = lrow(x, oc, 0, yl) + ke * ns + slot;
+    const word_t* pn = ((yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow(x, oc, 0, x.ny - 1)) + k * ns + slot;
+    const word_t* ps = ((yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow(x, oc, 0, 0)) + k * ns + slot;
+    int jo = y * hL + k, je = y * hL + ke, js = ys * hL + k;
+    word_t prev = valid ? x.sm[own + (L - 1) * zs] : 0;
+    word_t first = 0;
+    for (int z0 = 0; z0 < L; z0 += P) {
+      const int zd = z0 + (lane % P);
+      uint32_t um = 0;
+      if (col_ok && zd < L)
+        um = philox_draw(x.seed, (unsigned long long)(xx + L * (y + L * zd)), draw);
+#pragma unroll 1
+      for (int zi = 0; zi < P; ++zi) {
+        const int z = z0 + zi;
+        if (z >= L) break;  // warp-uniform
+        const uint32_t u = __shfl_sync(0xffffffffu, um, cl * P + zi);
+        if (valid) {
+          const bool last = (z == L - 1);
+          const word_t si = x.sm[own];
+          const word_t sd = last ? first : x.sm[own + zs];
+          const word_t mw = __ldg(Jxc + jo) ^ x.sm[ow] ^ si;
+          const word_t me = __ldg(Jxo + je) ^ x.sm[oe] ^ si;
+          const word_t mn = __ldg(Jyc + jo) ^ *pn ^ si;
+          const word_t ms = __ldg(Jyo + js) ^ *ps ^ si;
+          const word_t mu = __ldg(Jzc + jo) ^ prev ^ si;
+          const word_t md = __ldg(Jzc + (last ? jo - (L - 1) * zg : jo + zg)) ^ sd ^ si;
+          word_t c0, c1, c2;
+          count6(mw, me, mn, ms, mu, md, c0, c1, c2);
+          const word_t nsw = si ^ ~ge_scalar(c0, c1, c2, prefix_count<6>(u, th));
+          x.sm[own] = nsw;
+          if (z == 0) first = nsw;
+          prev = nsw;
+        }
+        own += zs;
+        ow += zs;
+        oe += zs;
+        pn += zs;
+        ps += zs;
+        jo += zg;
+        je += zg;
+        js += zg;
+      }
+    }
+  }
+}
+
+// Partial satisfied-bond counts of slots a..a+nsl-1 over this CTA's sites
+// (each bond counted once, from its site towards -x/-y/-z) into cnt[q][j].
+__device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, int a, int nsl,
+                                         unsigned (*cnt)[64]) {
+  for (int i = threadIdx.x; i < 128; i += blockDim.x) (&cnt[0][0])[i] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int per = 32 / nsl;
+  const int g = lane / nsl, slot = a + lane % nsl;
+  const int L = x.L, hL = x.hL, ns = x.ns;
+  const int cols = x.ny * hL;          // per colour per z
+  const int tot = 2 * x.zc * cols;     // local sites
+  const int zs = x.ny * x.rowW;
+  VCount<4> sm4;
+  VCount<16> big;
+  sm4.clear();
+  big.clear();
+  int it = 0;
+  for (int base = warp * per; base < tot; base += nwarps * per) {
+    const int t = base + g;
+    if (t < tot) {
+      // t -> (c, z, col)
+      const int cz = t / cols;          // c*zc + z (one division per site, measure only)
+      const int col = t - cz * cols;
+      const int c = cz / x.zc, z = cz - c * x.zc;
+      const int yl = div_hl(col, x);
+      const int k = col - yl * hL, y = x.y0 + yl;
+      const int par = (c + y) & 1, xx = 2 * k + par;
+      int kw, ke;
+      x_neighbours(k, par, hL, kw, ke);
+      const int oc = 1 - c;
+      const word_t si = x.sm[lrow(x, c, z, yl) + k * ns + slot];
+      const long jr = (long)(y + L * z) * hL + k;
+      const word_t w = (open && xx == 0) ? 0 : (__ldg(x.J + (long)(0 + c) * x.half + jr) ^ si ^
+                                                 x.sm[lrow(x, oc, z, yl) + kw * ns + slot]);
+      const word_t* pn = (yl > 0) ? x.sm + lrow(x, oc, z, yl - 1) : x.smN + lrow(x, oc, z, x.ny - 1);
+      const word_t n = __ldg(x.J + (long)(2 + c) * x.half + jr) ^ si ^ pn[k * ns + slot];
+      word_t q0, q1;
+      if (d3) {
+        const int zu = (z == 0) ? L - 1 : z - 1;
+        const word_t uu = __ldg(x.J + (long)(4 + c) * x.half + jr) ^ si ^ x.sm[lrow(x, c, zu, yl) + k * ns + slot];
+        q0 = w ^ n ^ uu;
+        q1 = (w & n) | (uu & (w ^ n));
+      } else {
+        q0 = w ^ n;
+        q1 = w & n;
+      }
+      add2_small(sm4, q0, q1);
+    }
+    if (++it == 5) {
+      add_small(big, sm4);
+      sm4.clear();
+      it = 0;
+    }
+  }
+  (void)zs;
+  add_small(big, sm4);
+  big.warp_sum_from(nsl);
+  const int q = lane % nsl;
+  for (int m = 0; m < 2 * nsl; ++m) {
+    const int j = (lane / nsl) + per * m;
+    atomicAdd(&cnt[q][j], big.count_of(j));
+  }
+}
+
+}  // namespace sa

@@ -14,6 +14,10 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
+# every batch test runs with the cluster-resident kernel and with the
+# global-memory kernel
+KERNELS = pytest.mark.parametrize("kernel", [0, 1], ids=["resident", "global"])
+
 
 def oracle_pt(lat, L, T, seed_J, seed, nsweeps, interval=1):
     systems = [O.OracleSystem(lat, L, mode=O.MODE_PHILOX) for _ in T]
@@ -43,11 +47,12 @@ def check_instance(b, i, lat, L, T, seed_J, seed, nsweeps, interval=1):
         assert np.array_equal(a, c)
 
 
+@KERNELS
 @pytest.mark.parametrize("nslots", [2, 3, 5, 8, 16, 32])
-def test_pt_batch_all_lane_classes(sab, nslots):
+def test_pt_batch_all_lane_classes(sab, nslots, kernel):
     from simulated_annealing_b200.batch import Batch
     T = list(np.geomspace(0.4, 2.1, nslots))
-    b = Batch()
+    b = Batch(kernel)
     lad = b.add_ladder(T)
     specs = [(O.LAT_2D, 6, 11), (O.LAT_2D_OPEN_X, 8, 12), (O.LAT_3D, 4, 13), (O.LAT_3D, 6, 14)]
     for lat, L, s in specs:
@@ -61,10 +66,12 @@ def test_pt_batch_all_lane_classes(sab, nslots):
         check_instance(b, i, lat, L, T, s, s + 50, 9)
 
 
-def test_c4_shapes_subset(sab):
-    """One instance of each C4 shape, 16 geometric slots, 12 sweeps."""
+@KERNELS
+def test_c4_shapes_subset(sab, kernel):
+    """One instance of each C4 shape, 16 geometric slots, 12 sweeps (the
+    resident kernel runs them in clusters of 1, 2, 4 and 8 CTAs)."""
     from simulated_annealing_b200.batch import Batch
-    b = Batch()
+    b = Batch(kernel)
     l2 = b.add_ladder(np.geomspace(0.3, 1.6, 16))
     l3 = b.add_ladder(np.geomspace(0.5, 2.0, 16))
     specs = [(O.LAT_2D, L, 1000 + k) for k, L in enumerate([16, 24, 32, 48, 64])]
@@ -80,10 +87,11 @@ def test_c4_shapes_subset(sab):
         check_instance(b, i, lat, L, list(T), s, s, 12)
 
 
-def test_exchange_interval(sab):
+@KERNELS
+def test_exchange_interval(sab, kernel):
     from simulated_annealing_b200.batch import Batch
     T = [0.5, 0.8, 1.3]
-    b = Batch()
+    b = Batch(kernel)
     lad = b.add_ladder(T)
     b.add_instance(O.LAT_3D, 4, ladder=lad, seed_J=3, seed=4)
     b.finalize()
@@ -94,12 +102,13 @@ def test_exchange_interval(sab):
     check_instance(b, 0, O.LAT_3D, 4, T, 3, 4, 9, interval=3)
 
 
-def test_anneal_instances_linear_schedule(sab):
+@KERNELS
+def test_anneal_instances_linear_schedule(sab, kernel):
     from simulated_annealing_b200.batch import Batch
     nsteps, per = 6, 5
     T0, T1 = 3.0, 0.2
     Ts = [T0 + (T1 - T0) * k / (nsteps - 1) for k in range(nsteps)]
-    b = Batch()
+    b = Batch(kernel)
     sch = b.add_schedule(Ts, per)
     specs = [(O.LAT_2D, 8, 21), (O.LAT_3D, 6, 22), (O.LAT_2D_OPEN_X, 10, 23)]
     for lat, L, s in specs:
@@ -132,3 +141,39 @@ def test_bad_instances_rejected(sab):
         b.add_instance(O.LAT_3D, 128, ladder=lad, seed_J=1, seed=1)
     with pytest.raises(SAError):
         b.add_ladder(np.linspace(1, 2, 33))
+
+
+@KERNELS
+def test_large_single_slot_anneal_uses_big_clusters(sab, kernel):
+    """3D L=32 and 2D L=128 single-slot anneals (serving-sized requests)."""
+    from simulated_annealing_b200.batch import Batch
+    Ts = [2.5, 1.5, 0.8]
+    b = Batch(kernel)
+    sch = b.add_schedule(Ts, 2)
+    specs = [(O.LAT_3D, 32, 41), (O.LAT_2D, 128, 42)]
+    for lat, L, s in specs:
+        b.add_instance(lat, L, schedule=sch, seed_J=s, seed=s)
+    b.finalize()
+    b.run(6)
+    b.sync()
+    for i, (lat, L, s) in enumerate(specs):
+        o = O.OracleSystem(lat, L, mode=O.MODE_PHILOX)
+        o.set_seed(s)
+        o.init_J()
+        o.set_seed(s)
+        o.init_rand()
+        for T in Ts:
+            o.set_T(T)
+            o.sweep(2)
+        assert np.array_equal(b.spins(i, 0), o.spins())
+
+
+def test_resident_groups(sab):
+    """The C4 mix needs one launch per (lanes-per-site, cluster size) group."""
+    from simulated_annealing_b200.batch import Batch
+    b = Batch()
+    lad = b.add_ladder(np.geomspace(0.5, 2.0, 16))
+    for L in (8, 12, 16, 20, 24):
+        b.add_instance(O.LAT_3D, L, ladder=lad, seed_J=L, seed=L)
+    b.finalize()
+    assert 1 <= b.launches_per_run() <= 5
