@@ -284,8 +284,10 @@ def run_ours(args):
 
     if rank == 0:
         peak, peak_src = measured_hbm_peak()
+        # the groups of one step run concurrently (one stream each): the unit
+        # of the roofline is the step's batched pass over every instance
         bytes_launch = algorithmic_bytes_per_sweep(insts) * S
-        launch_s = (ms / 1e3) / (args.steps * n_classes)
+        launch_s = (ms / 1e3) / args.steps
         achieved = bytes_launch / launch_s / 1e9
         tb, ts = profiled_traffic()
         traffic = (tb * S / ts) if (tb and ts) else None

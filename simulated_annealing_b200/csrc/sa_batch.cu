@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <random>
@@ -356,15 +357,22 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchParams p) {
 // ---------------------------------------------------------------------------
 // Shared-memory-resident kernel: one cluster of C CTAs per instance.
 // ---------------------------------------------------------------------------
-template <int P>
-__global__ void __launch_bounds__(kResThreads, 1) k_resident(BatchParams p) {
+// LAT: lattice kind of every instance of the launch; CL: clusters of more
+// than one CTA (DSMEM halos and cluster barriers) or single CTAs (block
+// barriers only).
+template <int P, int LAT, bool CL>
+__global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
   extern __shared__ __align__(16) word_t s_spins[];
   __shared__ unsigned s_cnt[2][64];   // this CTA's partial counts
   __shared__ unsigned s_tot[2][64];   // cluster totals
   __shared__ unsigned s_mask[2];
   cg::cluster_group cluster = cg::this_cluster();
-  const int C = (int)cluster.num_blocks();
-  const int q = (int)cluster.block_rank();
+  const int C = CL ? (int)cluster.num_blocks() : 1;
+  const int q = CL ? (int)cluster.block_rank() : 0;
+  auto sync_all = [&]() {
+    if (CL) cluster.sync();
+    else __syncthreads();
+  };
   const int id = p.order[blockIdx.x / C];
   const InstDesc d = p.inst[id];
   InstState* st = p.state + id;
@@ -378,7 +386,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(BatchParams p) {
   x.L = d.L;
   x.hL = d.L >> 1;
   x.ns = d.nslots;
-  x.zc = (d.lattice == SA_LATTICE_3D) ? d.L : 1;
+  x.zc = (LAT == SA_LATTICE_3D) ? d.L : 1;
   x.ny = d.L / C;
   x.y0 = q * x.ny;
   x.rowW = x.hL * x.ns;
@@ -386,10 +394,15 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(BatchParams p) {
   x.seed = d.seed;
   x.magic = (uint32_t)(0xFFFFFFFFu / (uint32_t)x.hL) + 1u;
   x.sm = s_spins;
-  x.smN = cluster.map_shared_rank(s_spins, (unsigned)((q + C - 1) % C));
-  x.smS = cluster.map_shared_rank(s_spins, (unsigned)((q + 1) % C));
+  if (CL) {
+    x.smN = cluster.map_shared_rank(s_spins, (unsigned)((q + C - 1) % C));
+    x.smS = cluster.map_shared_rank(s_spins, (unsigned)((q + 1) % C));
+  } else {
+    x.smN = s_spins;
+    x.smS = s_spins;
+  }
   x.J = p.J + d.J_off;
-  const bool d3 = d.lattice == SA_LATTICE_3D, open = d.lattice == SA_LATTICE_2D_OPEN_X;
+  constexpr bool d3 = LAT == SA_LATTICE_3D, open = LAT == SA_LATTICE_2D_OPEN_X;
 
   // global [colour][row = y + L*z][k][slot] -> local [colour][z][y_local][k][slot]
   word_t* gS = p.spins + d.spin_off;
@@ -400,7 +413,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(BatchParams p) {
     word_t* dst = s_spins + (long)cz * blk;
     for (int i = threadIdx.x; i < blk; i += blockDim.x) dst[i] = src[i];
   }
-  cluster.sync();
+  sync_all();
 
   const int lane = threadIdx.x & 31;
   const int slot = lane % P;
@@ -426,9 +439,8 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(BatchParams p) {
     }
     for (int c = 0; c < 2; ++c) {
       if (d3) rhalf_3d<P>(x, c, draw + c, th);
-      else if (open) rhalf_2d<P, true>(x, c, draw + c, th, tb);
-      else rhalf_2d<P, false>(x, c, draw + c, th, tb);
-      cluster.sync();
+      else rhalf_2d<P, open>(x, c, draw + c, th, tb);
+      sync_all();
     }
     draw += 2;
     const int64_t in_step = (d.sched >= 0) ? sweeps % d.sweeps_per_step : 0;
@@ -444,10 +456,14 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(BatchParams p) {
         nsl = 2;
       }
       rmeasure(x, d3, open, a, nsl, s_cnt);
-      cluster.sync();
+      sync_all();
       if (threadIdx.x < 128) {
         unsigned v = 0;
-        for (int r = 0; r < C; ++r) v += cluster.map_shared_rank(&s_cnt[0][0], (unsigned)r)[threadIdx.x];
+        if (CL) {
+          for (int r = 0; r < C; ++r) v += cluster.map_shared_rank(&s_cnt[0][0], (unsigned)r)[threadIdx.x];
+        } else {
+          v = (&s_cnt[0][0])[threadIdx.x];
+        }
         (&s_tot[0][0])[threadIdx.x] = v;
       }
       __syncthreads();
@@ -487,7 +503,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(BatchParams p) {
         st->elast[j] = e;
         st->emax[j] = (m0 == 0) ? e : max(st->emax[j], e);
       }
-      cluster.sync();
+      sync_all();
       if (meas && q == 0 && threadIdx.x == 0) st->measured += 1;
     }
   }
@@ -503,7 +519,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(BatchParams p) {
     st->sweeps = sweeps;
     st->xsteps = xsteps;
   }
-  cluster.sync();  // no CTA leaves while a peer may still read its shared memory
+  sync_all();  // no CTA leaves while a peer may still read its shared memory
 }
 
 // ---------------------------------------------------------------------------
@@ -632,8 +648,13 @@ struct sa_batch {
     bool resident;
     int P, C, begin, count, grid;
     size_t smem;
+    int threads;        // resident: block size matched to the shape's work
+    int lattice, L;     // resident groups hold one shape each
+    cudaStream_t stream;
+    cudaEvent_t done;
   };
   std::vector<Group> groups;
+  cudaEvent_t fork = nullptr;
   std::vector<int> cluster_of;  // per instance: C (0 = global-memory kernel)
 };
 
@@ -753,6 +774,17 @@ static int ensure_decisions(sa_batch* b, const std::vector<int64_t>& need) {
   return SA_OK;
 }
 
+// The resident kernel variant of a group: its lattice kind and whether its
+// clusters span several CTAs.
+template <int P>
+static void (*resident_kernel(const sa_batch::Group& g))(BatchParams) {
+  const bool cl = g.C > 1;
+  if (g.lattice == SA_LATTICE_3D) return cl ? k_resident<P, SA_LATTICE_3D, true> : k_resident<P, SA_LATTICE_3D, false>;
+  if (g.lattice == SA_LATTICE_2D_OPEN_X)
+    return cl ? k_resident<P, SA_LATTICE_2D_OPEN_X, true> : k_resident<P, SA_LATTICE_2D_OPEN_X, false>;
+  return cl ? k_resident<P, SA_LATTICE_2D, true> : k_resident<P, SA_LATTICE_2D, false>;
+}
+
 template <int P>
 static int launch_group(sa_batch* b, const sa_batch::Group& g, int gi, long nsweeps) {
   BatchParams p;
@@ -761,15 +793,15 @@ static int launch_group(sa_batch* b, const sa_batch::Group& g, int gi, long nswe
   p.ninst = g.count;
   p.work = b->d_work + gi;
   if (!g.resident) {
-    k_batch<P><<<g.grid, kBatchThreads, 0, b->stream>>>(p);
+    k_batch<P><<<g.grid, kBatchThreads, 0, g.stream>>>(p);
     SA_CUDA_TRY(cudaGetLastError());
     return SA_OK;
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(g.count * g.C), 1, 1);
-  cfg.blockDim = dim3(kResThreads, 1, 1);
+  cfg.blockDim = dim3((unsigned)g.threads, 1, 1);
   cfg.dynamicSmemBytes = g.smem;
-  cfg.stream = b->stream;
+  cfg.stream = g.stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = (unsigned)g.C;
@@ -777,17 +809,21 @@ static int launch_group(sa_batch* b, const sa_batch::Group& g, int gi, long nswe
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  SA_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_resident<P>, p));
+  SA_CUDA_TRY(cudaLaunchKernelEx(&cfg, resident_kernel<P>(g), p));
   return SA_OK;
 }
 
+// The per-kernel attributes are shared by every group of the same P, so the
+// dynamic shared-memory limit is the largest any such group needs
+// (`smem_limit`, set by the caller from all groups).
 template <int P>
-static int prepare_resident(const sa_batch::Group& g, int* max_clusters) {
-  SA_CUDA_TRY(cudaFuncSetAttribute(k_resident<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
-  if (g.C > 8) SA_CUDA_TRY(cudaFuncSetAttribute(k_resident<P>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+static int prepare_resident(const sa_batch::Group& g, size_t smem_limit, int* max_clusters) {
+  void (*kern)(BatchParams) = resident_kernel<P>(g);
+  SA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit));
+  SA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)g.C, 1, 1);
-  cfg.blockDim = dim3(kResThreads, 1, 1);
+  cfg.blockDim = dim3((unsigned)g.threads, 1, 1);
   cfg.dynamicSmemBytes = g.smem;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -796,14 +832,31 @@ static int prepare_resident(const sa_batch::Group& g, int* max_clusters) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  SA_CUDA_TRY(cudaOccupancyMaxActiveClusters(max_clusters, k_resident<P>, &cfg));
+  SA_CUDA_TRY(cudaOccupancyMaxActiveClusters(max_clusters, kern, &cfg));
+  if (*max_clusters < 1) {
+    cudaFuncAttributes fa;
+    cudaFuncGetAttributes(&fa, kern);
+    char buf[256];
+    snprintf(buf, sizeof buf,
+             "resident cluster not schedulable: P=%d C=%d threads=%d smem=%zu (kernel: %d regs, "
+             "max %d threads, %zu static smem, %d max dynamic smem)",
+             P, g.C, g.threads, g.smem, fa.numRegs, fa.maxThreadsPerBlock, fa.sharedSizeBytes,
+             fa.maxDynamicSharedSizeBytes);
+    return fail(SA_ERR_UNSUPPORTED, buf);
+  }
   return SA_OK;
 }
 
 template <int P>
 static int group_dispatch(sa_batch* b, const sa_batch::Group& g, int gi, long nsweeps, int prepare,
                           int* max_clusters) {
-  if (prepare) return g.resident ? prepare_resident<P>(g, max_clusters) : SA_OK;
+  if (prepare) {
+    if (!g.resident) return SA_OK;
+    size_t lim = 0;
+    for (const auto& o : b->groups)
+      if (o.resident && o.P == g.P && o.lattice == g.lattice && (o.C > 1) == (g.C > 1)) lim = std::max(lim, o.smem);
+    return prepare_resident<P>(g, lim, max_clusters);
+  }
   return launch_group<P>(b, g, gi, nsweeps);
 }
 
@@ -855,6 +908,11 @@ int sa_batch_destroy(sa_batch_t b) {
   cudaFree(b->d_stage);
   cudaFree(b->d_E);
   cudaFree(b->d_Eall);
+  for (auto& g : b->groups) {
+    if (g.stream) cudaStreamDestroy(g.stream);
+    if (g.done) cudaEventDestroy(g.done);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
   if (b->h_dec) cudaFreeHost(b->h_dec);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
   delete b;
@@ -972,6 +1030,9 @@ int sa_batch_finalize(sa_batch_t b) {
     if ((cx == 0) != (cy == 0)) return cx != 0;
     if (dx.P != dy.P) return dx.P < dy.P;
     if (cx != cy) return cx > cy;
+    if (cx != 0 && (dx.lattice != dy.lattice || dx.L != dy.L))
+      return dx.N * dx.nslots != dy.N * dy.nslots ? dx.N * dx.nslots > dy.N * dy.nslots
+                                                  : (dx.lattice != dy.lattice ? dx.lattice < dy.lattice : dx.L < dy.L);
     return dx.N * dx.nslots > dy.N * dy.nslots;
   });
   b->groups.clear();
@@ -979,9 +1040,30 @@ int sa_batch_finalize(sa_batch_t b) {
     const InstDesc& d = b->inst[order[i]];
     const int C = b->cluster_of[order[i]];
     const size_t smem = C ? (size_t)d.N * d.nslots * sizeof(word_t) / C : 0;
-    if (b->groups.empty() || b->groups.back().resident != (C != 0) || b->groups.back().P != d.P ||
-        b->groups.back().C != C) {
-      b->groups.push_back({C != 0, d.P, C, (int)i, 0, 0, 0});
+    const bool same = !b->groups.empty() && b->groups.back().resident == (C != 0) && b->groups.back().P == d.P &&
+                      b->groups.back().C == C &&
+                      (C == 0 || (b->groups.back().lattice == d.lattice && b->groups.back().L == d.L));
+    if (!same) {
+      sa_batch::Group g{};
+      g.resident = C != 0;
+      g.P = d.P;
+      g.C = C;
+      g.begin = (int)i;
+      g.lattice = d.lattice;
+      g.L = d.L;
+      g.threads = kBatchThreads;
+      if (C) {
+        // warp passes of one half-sweep: 3D walks columns, SPS = 32/P per pass;
+        // 2D takes tiles of 32 sites. Balance them over <= kResMaxWarps warps.
+        const int ny = d.L / C, hL = d.L / 2;
+        const int passes = (d.lattice == SA_LATTICE_3D) ? (ny * hL + (32 / d.P) - 1) / (32 / d.P)
+                                                        : (ny * hL + 31) / 32;
+        int warps = std::min(passes, kResMaxWarps);
+        const int rounds = (passes + warps - 1) / warps;
+        warps = std::max(4, (passes + rounds - 1) / rounds);
+        g.threads = warps * 32;
+      }
+      b->groups.push_back(g);
     }
     sa_batch::Group& g = b->groups.back();
     g.count += 1;
@@ -1020,13 +1102,15 @@ int sa_batch_finalize(sa_batch_t b) {
   b->h_xsteps.assign(ni, 0);
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  SA_CUDA_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
   for (size_t gi = 0; gi < b->groups.size(); ++gi) {
     sa_batch::Group& g = b->groups[gi];
+    SA_CUDA_TRY(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+    SA_CUDA_TRY(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
     if (g.resident) {
       int mc = 0;
       int st = dispatch(b, g, (int)gi, 0, 1, &mc);
       if (st) return st;
-      if (mc < 1) return fail(SA_ERR_UNSUPPORTED, "a resident cluster cannot be scheduled on this device");
       g.grid = mc;
     } else {
       g.grid = (int)std::min<int64_t>((int64_t)sms, (int64_t)g.count);  // one 512-thread CTA per SM
@@ -1105,10 +1189,17 @@ int sa_batch_run(sa_batch_t b, long nsweeps) {
   int st = ensure_decisions(b, need);
   if (st) return st;
   SA_CUDA_TRY(cudaMemsetAsync(b->d_work, 0, b->groups.size() * sizeof(int32_t), b->stream));
+  // every group on its own stream, forked from and joined back into the
+  // batch stream, so one group's tail overlaps the others' work
+  SA_CUDA_TRY(cudaEventRecord(b->fork, b->stream));
   for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    SA_CUDA_TRY(cudaStreamWaitEvent(b->groups[gi].stream, b->fork, 0));
     st = dispatch(b, b->groups[gi], (int)gi, nsweeps, 0, nullptr);
     if (st) return st;
+    SA_CUDA_TRY(cudaEventRecord(b->groups[gi].done, b->groups[gi].stream));
   }
+  for (size_t gi = 0; gi < b->groups.size(); ++gi)
+    SA_CUDA_TRY(cudaStreamWaitEvent(b->stream, b->groups[gi].done, 0));
   SA_CUDA_TRY(cudaGetLastError());
   return SA_OK;
 }

@@ -98,6 +98,36 @@ __device__ __forceinline__ void count6(word_t a, word_t b, word_t c, word_t d, w
 
 __device__ __forceinline__ word_t bcast(uint32_t bit) { return bit ? ~0ULL : 0ULL; }
 
+// Acceptance prefix t(u) = #{k in 0..7 : u < thr[k]} for a non-increasing
+// table with thr[7] == 0 (unused tail entries are 0): three comparisons of a
+// binary search, returned as the bits of t broadcast to 32-bit masks.
+__device__ __forceinline__ void prefix_bits(uint32_t u, const uint32_t* thr, uint32_t& m0, uint32_t& m1,
+                                            uint32_t& m2) {
+  const bool b2 = u < thr[3];
+  const bool b1 = u < (b2 ? thr[5] : thr[1]);
+  const bool b0 = u < (b2 ? (b1 ? thr[6] : thr[4]) : (b1 ? thr[2] : thr[0]));
+  m0 = b0 ? 0xFFFFFFFFu : 0u;
+  m1 = b1 ? 0xFFFFFFFFu : 0u;
+  m2 = b2 ? 0xFFFFFFFFu : 0u;
+}
+
+// New spin word: every replica whose satisfied-bond count (c2 c1 c0) is below
+// t (bits m2 m1 m0) flips. Evaluated on the 32-bit halves.
+__device__ __forceinline__ word_t flip_below(word_t s, word_t c0, word_t c1, word_t c2, uint32_t m0,
+                                             uint32_t m1, uint32_t m2) {
+  uint32_t r[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t a0 = (uint32_t)(c0 >> (32 * h)), a1 = (uint32_t)(c1 >> (32 * h));
+    const uint32_t a2 = (uint32_t)(c2 >> (32 * h)), sh = (uint32_t)(s >> (32 * h));
+    const uint32_t g0 = a0 | ~m0;
+    const uint32_t g1 = (a1 & ~m1) | (~(a1 ^ m1) & g0);
+    const uint32_t ge = (a2 & ~m2) | (~(a2 ^ m2) & g1);
+    r[h] = sh ^ ~ge;
+  }
+  return (word_t)r[0] | ((word_t)r[1] << 32);
+}
+
 // Mask of replicas whose bit-sliced count (c2 c1 c0) is >= the scalar t (0..7).
 __device__ __forceinline__ word_t ge_scalar(word_t c0, word_t c1, word_t c2, uint32_t t) {
   word_t t0 = bcast(t & 1), t1 = bcast(t & 2), t2 = bcast(t & 4);

@@ -23,7 +23,8 @@ namespace sa {
 
 namespace cg = cooperative_groups;
 
-constexpr int kResThreads = 512;
+constexpr int kResMaxWarps = 20;  // 5 warps per SM sub-partition at <= 96 registers
+constexpr int kResMaxThreads = kResMaxWarps * 32;
 
 struct ResCtx {
   word_t* sm;           // this CTA's rows
@@ -101,8 +102,9 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
         }
         word_t c0, c1, c2;
         count4(mw, me, mn, ms, c0, c1, c2);
-        const uint32_t tt = (OPEN_X && border) ? prefix_count<4>(u, tb) : prefix_count<4>(u, th);
-        x.sm[own] = si ^ ~ge_scalar(c0, c1, c2, tt);
+        uint32_t m0, m1, m2;
+        prefix_bits(u, (OPEN_X && border) ? tb : th, m0, m1, m2);
+        x.sm[own] = flip_below(si, c0, c1, c2, m0, m1, m2);
       }
     }
   }
@@ -149,7 +151,7 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
       uint32_t um = 0;
       if (col_ok && zd < L)
         um = philox_draw(x.seed, (unsigned long long)(xx + L * (y + L * zd)), draw);
-#pragma unroll 1
+#pragma unroll 2
       for (int zi = 0; zi < P; ++zi) {
         const int z = z0 + zi;
         if (z >= L) break;  // warp-uniform
@@ -166,7 +168,9 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
           const word_t md = __ldg(Jzc + (last ? jo - (L - 1) * zg : jo + zg)) ^ sd ^ si;
           word_t c0, c1, c2;
           count6(mw, me, mn, ms, mu, md, c0, c1, c2);
-          const word_t nsw = si ^ ~ge_scalar(c0, c1, c2, prefix_count<6>(u, th));
+          uint32_t m0, m1, m2;
+          prefix_bits(u, th, m0, m1, m2);
+          const word_t nsw = flip_below(si, c0, c1, c2, m0, m1, m2);
           x.sm[own] = nsw;
           if (z == 0) first = nsw;
           prev = nsw;
@@ -195,20 +199,20 @@ __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, in
   const int g = lane / nsl, slot = a + lane % nsl;
   const int L = x.L, hL = x.hL, ns = x.ns;
   const int cols = x.ny * hL;          // per colour per z
-  const int tot = 2 * x.zc * cols;     // local sites
-  const int zs = x.ny * x.rowW;
   VCount<4> sm4;
   VCount<16> big;
   sm4.clear();
   big.clear();
   int it = 0;
-  for (int base = warp * per; base < tot; base += nwarps * per) {
-    const int t = base + g;
-    if (t < tot) {
-      // t -> (c, z, col)
-      const int cz = t / cols;          // c*zc + z (one division per site, measure only)
-      const int col = t - cz * cols;
-      const int c = cz / x.zc, z = cz - c * x.zc;
+  const int tiles = (cols + per - 1) / per;      // site tiles per (colour, z)
+  const int units = 2 * x.zc * tiles;
+  // warp w takes the contiguous units [u0, u1) and walks (cz, tile) without division
+  const int u0 = (int)(((long)units * warp) / nwarps), u1 = (int)(((long)units * (warp + 1)) / nwarps);
+  int cz = u0 / tiles, tile = u0 - cz * tiles;
+  for (int un = u0; un < u1; ++un) {
+    const int col = tile * per + g;
+    if (col < cols) {
+      const int c = (cz >= x.zc) ? 1 : 0, z = cz - c * x.zc;
       const int yl = div_hl(col, x);
       const int k = col - yl * hL, y = x.y0 + yl;
       const int par = (c + y) & 1, xx = 2 * k + par;
@@ -233,13 +237,16 @@ __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, in
       }
       add2_small(sm4, q0, q1);
     }
+    if (++tile == tiles) {
+      tile = 0;
+      ++cz;
+    }
     if (++it == 5) {
       add_small(big, sm4);
       sm4.clear();
       it = 0;
     }
   }
-  (void)zs;
   add_small(big, sm4);
   big.warp_sum_from(nsl);
   const int q = lane % nsl;
