@@ -118,6 +118,25 @@ int sa_sys_sync(sa_system_t sys);
 int sa_sys_save(sa_system_t sys, void* buf, size_t cap, size_t* len);
 int sa_sys_load(sa_system_t sys, const void* buf, size_t len);
 
+/* Allocation-free energy measurement (no counterpart in the reference; the
+ * reference measures through its system object, which owns its buffers).
+ * Same result as sa_sys_measure -- E[j], M[j] per replica bit j -- for a
+ * lattice whose spins and own couplings the caller already holds on the
+ * device in the internal layout (see sa_sys_device_buffers), written to the
+ * caller's DEVICE arrays d_E[64], d_M[64], asynchronously on `stream`.
+ * For callers that cannot allocate device memory when they need an energy
+ * (a process that reserved its HBM budget up front, or a loop that cannot
+ * afford cudaMalloc's latency and implicit synchronisation): it calls no
+ * allocator. Its scratch is a fixed 256 KB array in the library's device
+ * image (512 partials of 128 counters), present on every device that loads
+ * the library until the process exits; lattices above 67,108,864 sites are
+ * rejected with SA_ERR_BUDGET. The first call on a device looks up the
+ * array's device address, so make that first call before any stream
+ * capture. All calls share the array: calls that overlap on the GPU (e.g. on
+ * two streams) race and must be ordered by the caller. */
+int sa_measure_noalloc(int lattice, int L, const uint64_t* d_spins, const uint64_t* d_J,
+                       int64_t* d_E, int64_t* d_M, void* stream);
+
 /* Device pointers of the internal layout (read-only use by advanced callers):
  * spins [colour][row][k] and own couplings [axis][colour][row][k]. */
 int sa_sys_device_buffers(sa_system_t sys, uint64_t** d_spins, uint64_t** d_J);

@@ -77,6 +77,7 @@ _PROTOS = {
     "sa_sys_save": (_c.c_int, [_vp, _vp, _c.c_size_t, _szp]),
     "sa_sys_load": (_c.c_int, [_vp, _vp, _c.c_size_t]),
     "sa_sys_device_buffers": (_c.c_int, [_vp, _c.POINTER(_u64p), _c.POINTER(_u64p)]),
+    "sa_measure_noalloc": (_c.c_int, [_c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _LIB = None

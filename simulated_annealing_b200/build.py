@@ -15,7 +15,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libsa_b200.so")
 
-SOURCES = ["sa_host.cpp", "sa_system.cu", "sa_batch.cu", "sa_runners.cu"]
+SOURCES = ["sa_host.cpp", "sa_system.cu", "sa_batch.cu", "sa_runners.cu", "sa_noalloc.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
