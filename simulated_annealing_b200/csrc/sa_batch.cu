@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchParams p) {
 // LAT: lattice kind of every instance of the launch; CL: clusters of more
 // than one CTA (DSMEM halos and cluster barriers) or single CTAs (block
 // barriers only).
-template <int P, int LAT, bool CL>
+template <int P, int SL, int LAT, bool CL>
 __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
   extern __shared__ __align__(16) word_t s_spins[];
   __shared__ unsigned s_cnt[2][64];   // this CTA's partial counts
@@ -416,13 +416,16 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
   sync_all();
 
   const int lane = threadIdx.x & 31;
-  const int slot = lane % P;
-  uint32_t th[8], tb[8];
+  const int slot = (lane % P) * SL;
+  uint32_t th[SL][8], tb[SL][8];
   int64_t step = -1;
   if (d.sched < 0) {
-    const BThr* t = p.thr + d.thr_off + (slot < d.nslots ? slot : 0);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) { th[k] = t->dn[k]; tb[k] = t->bdn[k]; }
+    for (int q = 0; q < SL; ++q) {
+      const BThr* t = p.thr + d.thr_off + (slot + q < d.nslots ? slot + q : 0);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { th[q][k] = t->dn[k]; tb[q][k] = t->bdn[k]; }
+    }
   }
   uint64_t draw = draw0;
   int64_t sweeps = sweeps0, xsteps = xsteps0;
@@ -434,12 +437,14 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
         step = s;
         const BThr* t = p.thr + d.thr_off + s;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) { th[k] = t->dn[k]; tb[k] = t->bdn[k]; }
+        for (int q = 0; q < SL; ++q)
+#pragma unroll
+          for (int k = 0; k < 8; ++k) { th[q][k] = t->dn[k]; tb[q][k] = t->bdn[k]; }
       }
     }
     for (int c = 0; c < 2; ++c) {
-      if (d3) rhalf_3d<P>(x, c, draw + c, th);
-      else rhalf_2d<P, open>(x, c, draw + c, th, tb);
+      if (d3) rhalf_3d<P, SL>(x, c, draw + c, th);
+      else rhalf_2d<P, SL, open>(x, c, draw + c, th, tb);
       sync_all();
     }
     draw += 2;
@@ -650,6 +655,7 @@ struct sa_batch {
     size_t smem;
     int threads;        // resident: block size matched to the shape's work
     int lattice, L;     // resident groups hold one shape each
+    int SL, RP;         // resident: slots per lane and lanes per site
     cudaStream_t stream;
     cudaEvent_t done;
   };
@@ -658,9 +664,9 @@ struct sa_batch {
   std::vector<int> cluster_of;  // per instance: C (0 = global-memory kernel)
 };
 
-// Shared-memory budget of one CTA of the resident kernel (the rest of the
-// 227 KB opt-in limit holds its static arrays).
-constexpr size_t kResSmemBudget = 224 * 1024;
+// Shared-memory budget of one CTA of the resident kernel: the 227 KB opt-in
+// limit minus room for its static arrays (counters, per-warp planes).
+constexpr size_t kResSmemBudget = 232448 - 8192;
 
 // Smallest cluster size C dividing L whose per-CTA share of the instance's
 // spins fits the budget; 0 if none does (the instance then runs in the
@@ -776,13 +782,30 @@ static int ensure_decisions(sa_batch* b, const std::vector<int64_t>& need) {
 
 // The resident kernel variant of a group: its lattice kind and whether its
 // clusters span several CTAs.
+template <int P, int SL>
+static void (*resident_kernel_sl(const sa_batch::Group& g))(BatchParams) {
+  const bool cl = g.C > 1;
+  if (g.lattice == SA_LATTICE_3D)
+    return cl ? k_resident<P, SL, SA_LATTICE_3D, true> : k_resident<P, SL, SA_LATTICE_3D, false>;
+  if (g.lattice == SA_LATTICE_2D_OPEN_X)
+    return cl ? k_resident<P, SL, SA_LATTICE_2D_OPEN_X, true> : k_resident<P, SL, SA_LATTICE_2D_OPEN_X, false>;
+  return cl ? k_resident<P, SL, SA_LATTICE_2D, true> : k_resident<P, SL, SA_LATTICE_2D, false>;
+}
+
+// Resident groups carry their own lanes-per-site RP and slots-per-lane SL
+// (RP * SL >= nslots); P (the instance descriptor's) is for the global kernel.
 template <int P>
 static void (*resident_kernel(const sa_batch::Group& g))(BatchParams) {
-  const bool cl = g.C > 1;
-  if (g.lattice == SA_LATTICE_3D) return cl ? k_resident<P, SA_LATTICE_3D, true> : k_resident<P, SA_LATTICE_3D, false>;
-  if (g.lattice == SA_LATTICE_2D_OPEN_X)
-    return cl ? k_resident<P, SA_LATTICE_2D_OPEN_X, true> : k_resident<P, SA_LATTICE_2D_OPEN_X, false>;
-  return cl ? k_resident<P, SA_LATTICE_2D, true> : k_resident<P, SA_LATTICE_2D, false>;
+  if (g.SL == 2) {
+    switch (g.RP) {
+      case 1: return resident_kernel_sl<1, 2>(g);
+      case 2: return resident_kernel_sl<2, 2>(g);
+      case 4: return resident_kernel_sl<4, 2>(g);
+      case 8: return resident_kernel_sl<8, 2>(g);
+      default: return resident_kernel_sl<16, 2>(g);
+    }
+  }
+  return resident_kernel_sl<P, 1>(g);
 }
 
 template <int P>
@@ -854,7 +877,9 @@ static int group_dispatch(sa_batch* b, const sa_batch::Group& g, int gi, long ns
     if (!g.resident) return SA_OK;
     size_t lim = 0;
     for (const auto& o : b->groups)
-      if (o.resident && o.P == g.P && o.lattice == g.lattice && (o.C > 1) == (g.C > 1)) lim = std::max(lim, o.smem);
+      if (o.resident && o.P == g.P && o.SL == g.SL && o.RP == g.RP && o.lattice == g.lattice &&
+          (o.C > 1) == (g.C > 1))
+        lim = std::max(lim, o.smem);
     return prepare_resident<P>(g, lim, max_clusters);
   }
   return launch_group<P>(b, g, gi, nsweeps);
@@ -1052,12 +1077,27 @@ int sa_batch_finalize(sa_batch_t b) {
       g.lattice = d.lattice;
       g.L = d.L;
       g.threads = kBatchThreads;
+      g.SL = 1;
+      g.RP = d.P;
       if (C) {
-        // warp passes of one half-sweep: 3D walks columns, SPS = 32/P per pass;
-        // 2D takes tiles of 32 sites. Balance them over <= kResMaxWarps warps.
+        // warp passes of one half-sweep: 3D walks columns, 32/RP per pass; 2D
+        // takes tiles of 32 sites (RP sub-steps of 32/RP sites each). Two slots
+        // per lane (16-byte accesses, shared addressing and couplings) when the
+        // slot count is even and there is still work for >= 12 warps.
         const int ny = d.L / C, hL = d.L / 2;
-        const int passes = (d.lattice == SA_LATTICE_3D) ? (ny * hL + (32 / d.P) - 1) / (32 / d.P)
-                                                        : (ny * hL + 31) / 32;
+        auto passes_for = [&](int rp) {
+          return (d.lattice == SA_LATTICE_3D) ? (ny * hL + (32 / rp) - 1) / (32 / rp) : (ny * hL + 31) / 32;
+        };
+        if (d.nslots % 2 == 0) {
+          int rp2 = 1;
+          while (rp2 * 2 < d.nslots) rp2 <<= 1;
+          const int p2 = (d.lattice == SA_LATTICE_3D) ? passes_for(rp2) : passes_for(rp2) * rp2 / d.P;
+          if (p2 >= 12 || d.lattice != SA_LATTICE_3D) {
+            g.SL = 2;
+            g.RP = rp2;
+          }
+        }
+        const int passes = passes_for(g.RP);
         int warps = std::min(passes, kResMaxWarps);
         const int rounds = (passes + warps - 1) / warps;
         warps = std::max(4, (passes + rounds - 1) / rounds);

@@ -51,12 +51,40 @@ __device__ __forceinline__ int lrow(const ResCtx& x, int c, int z, int yl) {
   return ((c * x.zc + z) * x.ny + yl) * x.rowW;
 }
 
-template <int P, bool OPEN_X>
-__device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, const uint32_t* th,
-                                         const uint32_t* tb) {
+// SL consecutive slot words of one site (SL = 2: one 16-byte access).
+template <int SL>
+struct SlotWords {
+  word_t w[SL];
+};
+
+template <int SL>
+__device__ __forceinline__ SlotWords<SL> ldw(const word_t* p) {
+  SlotWords<SL> r;
+  if (SL == 2) {
+    const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p);
+    r.w[0] = v.x;
+    r.w[SL - 1] = v.y;
+  } else {
+    r.w[0] = p[0];
+  }
+  return r;
+}
+
+template <int SL>
+__device__ __forceinline__ void stw(word_t* p, const SlotWords<SL>& v) {
+  if (SL == 2) *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(v.w[0], v.w[SL - 1]);
+  else p[0] = v.w[0];
+}
+
+// Lanes: (site group lane/P, slots (lane%P)*SL .. +SL-1). All slots of a site
+// share the coupling loads and the site's Philox draw; SL > 1 requires an
+// even slot count (16-byte aligned slot pairs).
+template <int P, int SL, bool OPEN_X>
+__device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, const uint32_t (*th)[8],
+                                         const uint32_t (*tb)[8]) {
   constexpr int SPS = 32 / P;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int slot = lane % P;
+  const int slot = (lane % P) * SL;
   const bool slot_ok = slot < x.ns;
   const int tot = x.ny * x.hL;
   const int L = x.L, hL = x.hL, ns = x.ns;
@@ -90,31 +118,42 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
         const word_t* pn = (yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow(x, oc, 0, x.ny - 1);
         const word_t* ps = (yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow(x, oc, 0, 0);
         const int ys = (y == L - 1) ? 0 : y + 1;
-        const word_t si = x.sm[own];
-        word_t mw = __ldg(Jxc + y * hL + k) ^ x.sm[orow + kw * ns + slot] ^ si;
-        word_t me = __ldg(Jxo + y * hL + ke) ^ x.sm[orow + ke * ns + slot] ^ si;
-        const word_t mn = __ldg(Jyc + y * hL + k) ^ pn[k * ns + slot] ^ si;
-        const word_t ms = __ldg(Jyo + ys * hL + k) ^ ps[k * ns + slot] ^ si;
-        bool border = false;
-        if (OPEN_X) {
-          if (xx == 0) { mw = ~0ULL; border = true; }
-          if (xx == L - 1) { me = ~0ULL; border = true; }
+        const SlotWords<SL> si = ldw<SL>(x.sm + own);
+        const SlotWords<SL> sw = ldw<SL>(x.sm + orow + kw * ns + slot);
+        const SlotWords<SL> se = ldw<SL>(x.sm + orow + ke * ns + slot);
+        const SlotWords<SL> sn = ldw<SL>(pn + k * ns + slot);
+        const SlotWords<SL> ss = ldw<SL>(ps + k * ns + slot);
+        const word_t jw = __ldg(Jxc + y * hL + k), je = __ldg(Jxo + y * hL + ke);
+        const word_t jn = __ldg(Jyc + y * hL + k), js = __ldg(Jyo + ys * hL + k);
+        const bool border = OPEN_X && (xx == 0 || xx == L - 1);
+        SlotWords<SL> out;
+#pragma unroll
+        for (int q = 0; q < SL; ++q) {
+          word_t mw = jw ^ sw.w[q] ^ si.w[q];
+          word_t me = je ^ se.w[q] ^ si.w[q];
+          const word_t mn = jn ^ sn.w[q] ^ si.w[q];
+          const word_t ms = js ^ ss.w[q] ^ si.w[q];
+          if (OPEN_X) {
+            if (xx == 0) mw = ~0ULL;
+            if (xx == L - 1) me = ~0ULL;
+          }
+          word_t c0, c1, c2;
+          count4(mw, me, mn, ms, c0, c1, c2);
+          uint32_t m0, m1, m2;
+          prefix_bits(u, border ? tb[q] : th[q], m0, m1, m2);
+          out.w[q] = flip_below(si.w[q], c0, c1, c2, m0, m1, m2);
         }
-        word_t c0, c1, c2;
-        count4(mw, me, mn, ms, c0, c1, c2);
-        uint32_t m0, m1, m2;
-        prefix_bits(u, (OPEN_X && border) ? tb : th, m0, m1, m2);
-        x.sm[own] = flip_below(si, c0, c1, c2, m0, m1, m2);
+        stw<SL>(x.sm + own, out);
       }
     }
   }
 }
 
-template <int P>
-__device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, const uint32_t* th) {
+template <int P, int SL>
+__device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, const uint32_t (*th)[8]) {
   constexpr int SPS = 32 / P;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int slot = lane % P, cl = lane / P;
+  const int slot = (lane % P) * SL, cl = lane / P;
   const bool slot_ok = slot < x.ns;
   const int L = x.L, hL = x.hL, ns = x.ns;
   const int cols = x.ny * hL;
@@ -144,8 +183,9 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
     const word_t* pn = ((yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow(x, oc, 0, x.ny - 1)) + k * ns + slot;
     const word_t* ps = ((yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow(x, oc, 0, 0)) + k * ns + slot;
     int jo = y * hL + k, je = y * hL + ke, js = ys * hL + k;
-    word_t prev = valid ? x.sm[own + (L - 1) * zs] : 0;
-    word_t first = 0;
+    SlotWords<SL> prev = {};
+    if (valid) prev = ldw<SL>(x.sm + own + (L - 1) * zs);
+    SlotWords<SL> first = {};
     for (int z0 = 0; z0 < L; z0 += P) {
       const int zd = z0 + (lane % P);
       uint32_t um = 0;
@@ -158,20 +198,26 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         const uint32_t u = __shfl_sync(0xffffffffu, um, cl * P + zi);
         if (valid) {
           const bool last = (z == L - 1);
-          const word_t si = x.sm[own];
-          const word_t sd = last ? first : x.sm[own + zs];
-          const word_t mw = __ldg(Jxc + jo) ^ x.sm[ow] ^ si;
-          const word_t me = __ldg(Jxo + je) ^ x.sm[oe] ^ si;
-          const word_t mn = __ldg(Jyc + jo) ^ *pn ^ si;
-          const word_t ms = __ldg(Jyo + js) ^ *ps ^ si;
-          const word_t mu = __ldg(Jzc + jo) ^ prev ^ si;
-          const word_t md = __ldg(Jzc + (last ? jo - (L - 1) * zg : jo + zg)) ^ sd ^ si;
-          word_t c0, c1, c2;
-          count6(mw, me, mn, ms, mu, md, c0, c1, c2);
-          uint32_t m0, m1, m2;
-          prefix_bits(u, th, m0, m1, m2);
-          const word_t nsw = flip_below(si, c0, c1, c2, m0, m1, m2);
-          x.sm[own] = nsw;
+          const SlotWords<SL> si = ldw<SL>(x.sm + own);
+          const SlotWords<SL> sd = last ? first : ldw<SL>(x.sm + own + zs);
+          const SlotWords<SL> sw = ldw<SL>(x.sm + ow);
+          const SlotWords<SL> se = ldw<SL>(x.sm + oe);
+          const SlotWords<SL> sn = ldw<SL>(pn);
+          const SlotWords<SL> ss = ldw<SL>(ps);
+          const word_t jw = __ldg(Jxc + jo), je_ = __ldg(Jxo + je), jn = __ldg(Jyc + jo);
+          const word_t js_ = __ldg(Jyo + js), ju = __ldg(Jzc + jo);
+          const word_t jd = __ldg(Jzc + (last ? jo - (L - 1) * zg : jo + zg));
+          SlotWords<SL> nsw;
+#pragma unroll
+          for (int q = 0; q < SL; ++q) {
+            word_t c0, c1, c2;
+            count6(jw ^ sw.w[q] ^ si.w[q], je_ ^ se.w[q] ^ si.w[q], jn ^ sn.w[q] ^ si.w[q],
+                   js_ ^ ss.w[q] ^ si.w[q], ju ^ prev.w[q] ^ si.w[q], jd ^ sd.w[q] ^ si.w[q], c0, c1, c2);
+            uint32_t m0, m1, m2;
+            prefix_bits(u, th[q], m0, m1, m2);
+            nsw.w[q] = flip_below(si.w[q], c0, c1, c2, m0, m1, m2);
+          }
+          stw<SL>(x.sm + own, nsw);
           if (z == 0) first = nsw;
           prev = nsw;
         }
