@@ -118,6 +118,17 @@ int sa_sys_sync(sa_system_t sys);
 int sa_sys_save(sa_system_t sys, void* buf, size_t cap, size_t* len);
 int sa_sys_load(sa_system_t sys, const void* buf, size_t len);
 
+/* annealing<gpu_sys> on the device (src/annealing.hpp:67-100) for one system:
+ * nsteps steps, step k at temperature T[k] with `sweeps` sweeps, measuring
+ * after every sweep i (inside the step) with i % stride == 0 (stride 0: never)
+ * and keeping the running maximum of the float -H = E + h*M per replica
+ * (the reference's min_E) in min_E[64] (host). step_E (host, nsteps*64, may
+ * be NULL) receives the integer E of the last measurement of every step.
+ * The reference's geometric cooling T *= alfa is the schedule T[k] =
+ * T0*alfa^k. Leaves the system at temperature T[nsteps-1]. Synchronous. */
+int sa_sys_anneal(sa_system_t sys, const double* T, int nsteps, int sweeps, int stride, float* min_E,
+                  int64_t* step_E);
+
 /* Allocation-free energy measurement (no counterpart in the reference; the
  * reference measures through its system object, which owns its buffers).
  * Same result as sa_sys_measure -- E[j], M[j] per replica bit j -- for a

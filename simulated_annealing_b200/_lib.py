@@ -78,6 +78,7 @@ _PROTOS = {
     "sa_sys_load": (_c.c_int, [_vp, _vp, _c.c_size_t]),
     "sa_sys_device_buffers": (_c.c_int, [_vp, _c.POINTER(_u64p), _c.POINTER(_u64p)]),
     "sa_measure_noalloc": (_c.c_int, [_c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "sa_sys_anneal": (_c.c_int, [_vp, _f64p, _c.c_int, _c.c_int, _c.c_int, _f32p, _i64p]),
 }
 
 _LIB = None

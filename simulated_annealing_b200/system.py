@@ -130,6 +130,16 @@ class GpuSystem:
         buf = ctypes.create_string_buffer(data, len(data))
         check(self._lib.sa_sys_load(self._h, buf, len(data)))
 
+    def anneal(self, T, sweeps: int, stride: int = 1):
+        """annealing<gpu_sys> on the device over the schedule T (one entry per
+        step of `sweeps` sweeps). Returns (min_E float[64], step_E int64[nsteps, 64])."""
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        mn = np.zeros(64, dtype=np.float32)
+        stepE = np.zeros((len(T), 64), dtype=np.int64)
+        check(self._lib.sa_sys_anneal(self._h, _p(T, ctypes.c_double), len(T), int(sweeps), int(stride),
+                                      _p(mn, ctypes.c_float), _p(stepE, ctypes.c_int64)))
+        return mn, stepE
+
     # -- data access -----------------------------------------------------------
     def set_J(self, jx, jy, jz=None) -> None:
         jx = np.ascontiguousarray(jx, dtype=np.uint64)

@@ -150,3 +150,64 @@ def test_c1_prefix_bit_exact(sab):
     g.sweep(1000)
     o.sweep(1000)
     _check(g, o)
+
+
+def oracle_anneal(o, Ts, sweeps, stride):
+    """annealing<> over an explicit schedule, restated with the oracle system:
+    step k at Ts[k]; measure when i % stride == 0; running max of the float -H."""
+    mn = None
+    last = np.zeros((len(Ts), 64), dtype=np.float32)
+    res = np.zeros(64, dtype=np.float32)
+    for k, T in enumerate(Ts):
+        o.set_T(T)
+        for i in range(sweeps):
+            o.sweep(1)
+            if stride != 0 and i % stride == 0:
+                res = o.measure_float()
+                mn = res.copy() if mn is None else np.maximum(mn, res)
+        last[k] = res
+    return mn, last
+
+
+@pytest.mark.parametrize("lat,L,h", [(O.LAT_3D, 8, 0.0), (O.LAT_2D, 16, 0.3), (O.LAT_2D_OPEN_X, 12, 0.0)])
+def test_device_anneal_matches_annealing_template(sab, lat, L, h):
+    """sa_sys_anneal vs annealing<> restated by the oracle (linear schedule)."""
+    nsteps, sweeps = 9, 6
+    T0, T1 = 3.0, 0.2
+    Ts = [T0 + (T1 - T0) * k / (nsteps - 1) for k in range(nsteps)]
+    g, o = _pair(sab, lat, L, T0, h)
+    _setup((g, o), 1, 2)
+    mn, stepE = g.anneal(Ts, sweeps, 1)
+    ref, last = oracle_anneal(o, Ts, sweeps, 1)
+    assert np.array_equal(mn, ref)
+    assert np.array_equal(g.get_spins(), o.spins())
+    if h == 0.0:
+        assert np.array_equal(stepE.astype(np.float32), last)
+    # and the oracle's own C restatement of the template agrees for the same schedule
+    o2 = O.OracleSystem(lat, L, T0, h, O.MODE_PHILOX)
+    _setup((o2,), 1, 2)
+    ref2, _ = o2.anneal(T0, 1, T1, nsteps, sweeps, 1)
+    assert np.array_equal(ref, ref2)
+
+
+def test_device_anneal_stride_and_geometric(sab):
+    g, o = _pair(sab, O.LAT_3D, 6, 2.5, 0.0)
+    _setup((g, o), 4, 5)
+    Ts = [2.5 * 0.8 ** k for k in range(5)]
+    mn, _ = g.anneal(Ts, 7, 3)
+    ref, _ = oracle_anneal(o, Ts, 7, 3)
+    assert np.array_equal(mn, ref)
+    assert np.array_equal(g.get_spins(), o.spins())
+
+
+def test_c2_prefix(sab):
+    """C2 shape: 3D L=32, J seed 3, linear T 3.0 -> 0.2 over 200 steps of 100
+    sweeps; the first 3 steps against the oracle, per-step integer energies too."""
+    Ts = [3.0 + (0.2 - 3.0) * k / 199 for k in range(200)][:3]
+    g, o = _pair(sab, O.LAT_3D, 32, 3.0)
+    _setup((g, o), 3, 3)
+    mn, stepE = g.anneal(Ts, 100, 1)
+    ref_mn, ref_last = oracle_anneal(o, Ts, 100, 1)
+    assert np.array_equal(mn, ref_mn)
+    assert np.array_equal(stepE.astype(np.float32), ref_last)
+    assert np.array_equal(g.get_spins(), o.spins())
