@@ -118,6 +118,16 @@ int sa_sys_sync(sa_system_t sys);
 int sa_sys_save(sa_system_t sys, void* buf, size_t cap, size_t* len);
 int sa_sys_load(sa_system_t sys, const void* buf, size_t len);
 
+/* The exchange schedule of parallel_tempering<> for n temperatures
+ * (src/parallel_tempering.hpp:193-198, 251-253): std::mt19937(123) driving
+ * uniform_int_distribution<int>(0, n-2) then uniform_real_distribution<double>;
+ * entries skip .. skip+count-1 into pair[] and r[] (host). */
+int sa_pt_sequence(int n, long skip, long count, int32_t* pair, double* r);
+/* The reference's exchange mask for one pair (src/parallel_tempering.hpp:
+ * 141-162): bit j iff dE*dB > 0 || r < exp(dB*dE), dE = -(Ei[j]-Ej[j]) (float),
+ * dB = 1/Ti - 1/Tj. Host-only arithmetic. */
+uint64_t sa_pt_mask(const float* Ei, const float* Ej, double Ti, double Tj, double r);
+
 /* annealing<gpu_sys> on the device (src/annealing.hpp:67-100) for one system:
  * nsteps steps, step k at temperature T[k] with `sweeps` sweeps, measuring
  * after every sweep i (inside the step) with i % stride == 0 (stride 0: never)

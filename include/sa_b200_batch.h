@@ -51,6 +51,13 @@ int sa_batch_add_instance(sa_batch_t b, int lattice, int L, int ladder_id, int s
  * the device and uploads the tables. No instance may be added afterwards. */
 int sa_batch_finalize(sa_batch_t b);
 
+/* Energy histograms, before finalize: every `stride` sweeps (0 = off) every
+ * slot of every parallel-tempering instance is measured (before the
+ * exchange) and its 64 replica energies are binned on the device; bin b of a
+ * slot counts E = 2b - nbonds. Needs the resident kernel. */
+int sa_batch_set_histograms(sa_batch_t b, int stride);
+/* Histogram of one slot: *nbins = nbonds + 1; out (host) may be NULL. */
+int sa_batch_histogram(sa_batch_t b, int instance, int slot, int32_t* out, long cap, long* nbins);
 /* Kernel choice, before finalize: 0 (default) keeps every instance whose
  * spins fit in the shared memory of a cluster of <= 16 CTAs resident there for
  * a whole launch and runs the rest in the global-memory kernel; 1 runs every
@@ -104,6 +111,34 @@ int sa_batch_last_h2d_bytes(sa_batch_t b, long long* n);
 int sa_batch_anneal_result(sa_batch_t b, int instance, int64_t* Emax, long* sweeps_done);
 /* Sweeps done by an instance so far. */
 int sa_batch_sweeps_done(sa_batch_t b, int instance, long* sweeps_done);
+
+/* ---- serving: continuous batching of anneal requests ------------------------
+ * No reference counterpart: the reference runs one system per process
+ * (src/main.cpp). A server owns device pools sized from budget_bytes and
+ * admits a request (lattice, L, coupling seed, spin/RNG seed, schedule T[nsteps]
+ * of sweeps_per_step sweeps each) only when the pools have room; otherwise
+ * sa_serve_submit returns SA_ERR_BUDGET and the caller retries after
+ * collecting results. Each sa_serve_run call advances every active request by
+ * up to nsweeps sweeps in one set of launches (the batch kernels); requests
+ * join at the next call. A request's result depends only on its own
+ * parameters, never on what runs beside it. sa_serve_poll lists finished
+ * requests; sa_serve_result copies one out (after sa_serve_sync) and frees it.
+ */
+typedef struct sa_serve* sa_serve_t;
+
+int sa_serve_create(size_t budget_bytes, int max_requests, sa_serve_t* out);
+int sa_serve_destroy(sa_serve_t s);
+int sa_serve_set_stream(sa_serve_t s, void* stream);
+int sa_serve_submit(sa_serve_t s, int lattice, int L, uint64_t seed_J, uint64_t seed, const double* T, int nsteps,
+                    int sweeps_per_step, int64_t* id);
+int sa_serve_run(sa_serve_t s, long nsweeps);
+int sa_serve_sync(sa_serve_t s);
+int sa_serve_poll(sa_serve_t s, int64_t* ids, int cap, int* n);
+/* Emax: running max of -H per replica over the measurements (int64[64]);
+ * Elast: last measured -H (int64[64], may be NULL); spins: final row-major
+ * spin words (N of them, may be NULL). Frees the request. */
+int sa_serve_result(sa_serve_t s, int64_t id, int64_t* Emax, int64_t* Elast, uint64_t* spins);
+int sa_serve_active(sa_serve_t s, int* n, long long* free_words);
 
 #ifdef __cplusplus
 }

@@ -79,6 +79,8 @@ _PROTOS = {
     "sa_sys_device_buffers": (_c.c_int, [_vp, _c.POINTER(_u64p), _c.POINTER(_u64p)]),
     "sa_measure_noalloc": (_c.c_int, [_c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp]),
     "sa_sys_anneal": (_c.c_int, [_vp, _f64p, _c.c_int, _c.c_int, _c.c_int, _f32p, _i64p]),
+    "sa_pt_sequence": (_c.c_int, [_c.c_int, _c.c_long, _c.c_long, _i32p, _f64p]),
+    "sa_pt_mask": (_c.c_uint64, [_f32p, _f32p, _c.c_double, _c.c_double, _c.c_double]),
 }
 
 _LIB = None

@@ -34,6 +34,8 @@ for _name, _res, _args in [
     ("sa_batch_set_exchange_interval", _c.c_int, [_vp, _c.c_int]),
     ("sa_batch_set_measure_stride", _c.c_int, [_vp, _c.c_int]),
     ("sa_batch_set_kernel", _c.c_int, [_vp, _c.c_int]),
+    ("sa_batch_set_histograms", _c.c_int, [_vp, _c.c_int]),
+    ("sa_batch_histogram", _c.c_int, [_vp, _c.c_int, _c.c_int, _c.POINTER(_c.c_int32), _c.c_long, _lp]),
     ("sa_batch_launches_per_run", _c.c_int, [_vp, _ip]),
     ("sa_batch_record_exchanges", _c.c_int, [_vp, _c.c_long]),
     ("sa_batch_run", _c.c_int, [_vp, _c.c_long]),
@@ -111,6 +113,16 @@ class Batch:
 
     def set_exchange_interval(self, k: int) -> None:
         check(self._lib.sa_batch_set_exchange_interval(self._h, int(k)))
+
+    def set_histograms(self, stride: int) -> None:
+        check(self._lib.sa_batch_set_histograms(self._h, int(stride)))
+
+    def histogram(self, i: int, slot: int) -> np.ndarray:
+        n = _c.c_long()
+        check(self._lib.sa_batch_histogram(self._h, i, slot, None, 0, _c.byref(n)))
+        out = np.zeros(n.value, dtype=np.int32)
+        check(self._lib.sa_batch_histogram(self._h, i, slot, _p(out, _c.c_int32), n.value, _c.byref(n)))
+        return out
 
     def set_measure_stride(self, k: int) -> None:
         check(self._lib.sa_batch_set_measure_stride(self._h, int(k)))

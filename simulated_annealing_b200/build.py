@@ -14,6 +14,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libsa_b200.so")
+PLAIN = os.path.join(PKG, "sa_plain_pt")  # plain per-instance PT timing program (links LIB)
 
 SOURCES = ["sa_host.cpp", "sa_system.cu", "sa_batch.cu", "sa_runners.cu", "sa_noalloc.cu"]
 
@@ -44,12 +45,19 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-shared", "-o", LIB, *sources(), "-lcudart"]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+    if force or not up_to_date():
+        cmd = [nvcc(), *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-shared", "-o", LIB, *sources(), "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+    src = os.path.join(CSRC, "sa_plain_pt.cpp")
+    if force or not os.path.exists(PLAIN) or os.path.getmtime(PLAIN) < max(os.path.getmtime(src),
+                                                                            os.path.getmtime(LIB)):
+        cmd = [nvcc(), "-Wno-deprecated-gpu-targets", "-O2", "-std=c++17", "-I", INCLUDE, "-o", PLAIN, src, "-L", PKG, "-lsa_b200",
+               "-Xlinker", "-rpath,$ORIGIN", "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
     return LIB
 
 

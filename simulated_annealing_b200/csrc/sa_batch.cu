@@ -246,7 +246,7 @@ __device__ void measure_slots(const InstDesc& d, const word_t* __restrict__ S,
 template <int P>
 __device__ void run_instance(const BatchParams& p, const InstDesc& d, int id, unsigned (*cnt)[64],
                              unsigned* smask) {
-  InstState* st = p.state + id;
+  InstState* st = p.state + d.state_idx;
   uint64_t draw = st->draw;
   int64_t sweeps = st->sweeps, xsteps = st->xsteps;
   int64_t n = p.nsweeps;
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
   };
   const int id = p.order[blockIdx.x / C];
   const InstDesc d = p.inst[id];
-  InstState* st = p.state + id;
+  InstState* st = p.state + d.state_idx;
   const uint64_t draw0 = st->draw;
   const int64_t sweeps0 = st->sweeps, xsteps0 = st->xsteps;
   int64_t n = p.nsweeps;
@@ -450,6 +450,27 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
     draw += 2;
     const int64_t in_step = (d.sched >= 0) ? sweeps % d.sweeps_per_step : 0;
     sweeps += 1;
+    // energy histograms of every slot, taken before the exchange (the energies
+    // the reference's PT step measures, src/parallel_tempering.hpp:85-95)
+    if (p.hist && d.hist_off >= 0 && sweeps % p.hstride == 0) {
+      for (int a = 0; a < d.nslots; a += 2) {
+        const int nh = (a + 1 < d.nslots) ? 2 : 1;
+        rmeasure(x, d3, open, a, nh, s_cnt);
+        sync_all();
+        if (q == 0 && threadIdx.x < 64 * nh) {
+          const int qq = threadIdx.x >> 6, j = threadIdx.x & 63;
+          unsigned v = 0;
+          if (CL) {
+            for (int r = 0; r < C; ++r) v += cluster.map_shared_rank(&s_cnt[0][0], (unsigned)r)[qq * 64 + j];
+          } else {
+            v = s_cnt[qq][j];
+          }
+          // E = 2v - nbonds -> bin (E + nbonds) / 2 = v
+          atomicAdd(&p.hist[d.hist_off + (long)(a + qq) * (d.nbonds + 1) + v], 1);
+        }
+        sync_all();
+      }
+    }
     const bool xchg = d.ladder >= 0 && d.nslots > 1 && sweeps % p.xinterval == 0;
     const bool meas = d.sched >= 0 && p.mstride > 0 && in_step % p.mstride == 0;
     if (xchg || meas) {
@@ -645,8 +666,14 @@ struct sa_batch {
   int64_t h_dec_cap = 0;
   int64_t h2d_bytes_last = 0;  // host->device bytes of the last sa_batch_run
   int64_t* d_Eall = nullptr;   // all-slot energies
+  size_t inst_cap = 0;         // serving: capacity of d_inst / d_order / d_seedJ
+  size_t work_cap = 0;         // serving: capacity of d_work
+  uint64_t* d_seedJ = nullptr; // serving: seeds of the requests being initialised
   int64_t e_count = 0;         // sum of nslots*64
   bool force_global = false;   // run every instance in the global-memory kernel
+  int hstride = 0;             // energy histograms every hstride sweeps (0 = off)
+  int32_t* d_hist = nullptr;
+  int64_t hist_count = 0;
   // Launch groups: a contiguous range of the work order sharing the kernel
   // (resident or global), the lanes-per-site P and the cluster size C.
   struct Group {
@@ -684,6 +711,8 @@ static int choose_cluster(const InstDesc& d) {
 template <int P>
 static int launch_group(sa_batch* b, const sa_batch::Group& g, int gi, long nsweeps);
 
+static std::vector<int32_t> build_groups(sa_batch* b);
+
 static BThr to_bthr(int lattice, double T) {
   Thresholds t;
   make_thresholds(lattice, T, 0.0, &t);
@@ -711,7 +740,80 @@ static int batch_params(sa_batch* b, long nsweeps, BatchParams* p) {
   p->nsweeps = nsweeps;
   p->xinterval = b->xinterval;
   p->mstride = b->mstride;
+  p->hist = b->d_hist;
+  p->hstride = b->hstride > 0 ? b->hstride : 1;
   return SA_OK;
+}
+
+// Work order and launch groups of the current instance table: grouped by
+// (kernel, lanes-per-site, cluster size, shape), most expensive first.
+static std::vector<int32_t> build_groups(sa_batch* b) {
+  // work order: grouped by (kernel, P, C), most expensive first inside a group
+  b->cluster_of.resize(b->inst.size());
+  for (size_t i = 0; i < b->inst.size(); ++i) b->cluster_of[i] = b->force_global ? 0 : choose_cluster(b->inst[i]);
+  std::vector<int32_t> order(b->inst.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int32_t)i;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+    const InstDesc &dx = b->inst[x], &dy = b->inst[y];
+    const int cx = b->cluster_of[x], cy = b->cluster_of[y];
+    if ((cx == 0) != (cy == 0)) return cx != 0;
+    if (dx.P != dy.P) return dx.P < dy.P;
+    if (cx != cy) return cx > cy;
+    if (cx != 0 && (dx.lattice != dy.lattice || dx.L != dy.L))
+      return dx.N * dx.nslots != dy.N * dy.nslots ? dx.N * dx.nslots > dy.N * dy.nslots
+                                                  : (dx.lattice != dy.lattice ? dx.lattice < dy.lattice : dx.L < dy.L);
+    return dx.N * dx.nslots > dy.N * dy.nslots;
+  });
+  b->groups.clear();
+  for (size_t i = 0; i < order.size(); ++i) {
+    const InstDesc& d = b->inst[order[i]];
+    const int C = b->cluster_of[order[i]];
+    const size_t smem = C ? (size_t)d.N * d.nslots * sizeof(word_t) / C : 0;
+    const bool same = !b->groups.empty() && b->groups.back().resident == (C != 0) && b->groups.back().P == d.P &&
+                      b->groups.back().C == C &&
+                      (C == 0 || (b->groups.back().lattice == d.lattice && b->groups.back().L == d.L));
+    if (!same) {
+      sa_batch::Group g{};
+      g.resident = C != 0;
+      g.P = d.P;
+      g.C = C;
+      g.begin = (int)i;
+      g.lattice = d.lattice;
+      g.L = d.L;
+      g.threads = kBatchThreads;
+      g.SL = 1;
+      g.RP = d.P;
+      if (C) {
+        // warp passes of one half-sweep: 3D walks columns, 32/RP per pass; 2D
+        // takes tiles of 32 sites (RP sub-steps of 32/RP sites each). Two slots
+        // per lane (16-byte accesses, shared addressing and couplings) when the
+        // slot count is even and there is still work for >= 12 warps.
+        const int ny = d.L / C, hL = d.L / 2;
+        auto passes_for = [&](int rp) {
+          return (d.lattice == SA_LATTICE_3D) ? (ny * hL + (32 / rp) - 1) / (32 / rp) : (ny * hL + 31) / 32;
+        };
+        if (d.nslots % 2 == 0) {
+          int rp2 = 1;
+          while (rp2 * 2 < d.nslots) rp2 <<= 1;
+          const int p2 = (d.lattice == SA_LATTICE_3D) ? passes_for(rp2) : passes_for(rp2) * rp2 / d.P;
+          if (p2 >= 12 || d.lattice != SA_LATTICE_3D) {
+            g.SL = 2;
+            g.RP = rp2;
+          }
+        }
+        const int passes = passes_for(g.RP);
+        int warps = std::min(passes, kResMaxWarps);
+        const int rounds = (passes + warps - 1) / warps;
+        warps = std::max(4, (passes + rounds - 1) / rounds);
+        g.threads = warps * 32;
+      }
+      b->groups.push_back(g);
+    }
+    sa_batch::Group& g = b->groups.back();
+    g.count += 1;
+    g.smem = std::max(g.smem, smem);
+  }
+  return order;
 }
 
 // Extends every ladder's exchange table to cover `need` attempts. Each
@@ -933,6 +1035,8 @@ int sa_batch_destroy(sa_batch_t b) {
   cudaFree(b->d_stage);
   cudaFree(b->d_E);
   cudaFree(b->d_Eall);
+  cudaFree(b->d_hist);
+  cudaFree(b->d_seedJ);
   for (auto& g : b->groups) {
     if (g.stream) cudaStreamDestroy(g.stream);
     if (g.done) cudaEventDestroy(g.done);
@@ -1009,6 +1113,7 @@ int sa_batch_add_instance(sa_batch_t b, int lattice, int L, int ladder, int sche
     Ladder& ld = b->ladders[ladder];
     ld.span = std::max<int64_t>(ld.span, 2 * d.nbonds);
   }
+  d.state_idx = (int64_t)b->inst.size();
   b->inst.push_back(d);
   b->seed_J.push_back(seed_J);
   *id = (int)b->inst.size() - 1;
@@ -1044,71 +1149,23 @@ int sa_batch_finalize(sa_batch_t b) {
     d.thr_off = it->second;
   }
   b->npairs = pair_off;
-  // work order: grouped by (kernel, P, C), most expensive first inside a group
-  b->cluster_of.resize(b->inst.size());
-  for (size_t i = 0; i < b->inst.size(); ++i) b->cluster_of[i] = b->force_global ? 0 : choose_cluster(b->inst[i]);
-  std::vector<int32_t> order(b->inst.size());
-  for (size_t i = 0; i < order.size(); ++i) order[i] = (int32_t)i;
-  std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
-    const InstDesc &dx = b->inst[x], &dy = b->inst[y];
-    const int cx = b->cluster_of[x], cy = b->cluster_of[y];
-    if ((cx == 0) != (cy == 0)) return cx != 0;
-    if (dx.P != dy.P) return dx.P < dy.P;
-    if (cx != cy) return cx > cy;
-    if (cx != 0 && (dx.lattice != dy.lattice || dx.L != dy.L))
-      return dx.N * dx.nslots != dy.N * dy.nslots ? dx.N * dx.nslots > dy.N * dy.nslots
-                                                  : (dx.lattice != dy.lattice ? dx.lattice < dy.lattice : dx.L < dy.L);
-    return dx.N * dx.nslots > dy.N * dy.nslots;
-  });
-  b->groups.clear();
-  for (size_t i = 0; i < order.size(); ++i) {
-    const InstDesc& d = b->inst[order[i]];
-    const int C = b->cluster_of[order[i]];
-    const size_t smem = C ? (size_t)d.N * d.nslots * sizeof(word_t) / C : 0;
-    const bool same = !b->groups.empty() && b->groups.back().resident == (C != 0) && b->groups.back().P == d.P &&
-                      b->groups.back().C == C &&
-                      (C == 0 || (b->groups.back().lattice == d.lattice && b->groups.back().L == d.L));
-    if (!same) {
-      sa_batch::Group g{};
-      g.resident = C != 0;
-      g.P = d.P;
-      g.C = C;
-      g.begin = (int)i;
-      g.lattice = d.lattice;
-      g.L = d.L;
-      g.threads = kBatchThreads;
-      g.SL = 1;
-      g.RP = d.P;
-      if (C) {
-        // warp passes of one half-sweep: 3D walks columns, 32/RP per pass; 2D
-        // takes tiles of 32 sites (RP sub-steps of 32/RP sites each). Two slots
-        // per lane (16-byte accesses, shared addressing and couplings) when the
-        // slot count is even and there is still work for >= 12 warps.
-        const int ny = d.L / C, hL = d.L / 2;
-        auto passes_for = [&](int rp) {
-          return (d.lattice == SA_LATTICE_3D) ? (ny * hL + (32 / rp) - 1) / (32 / rp) : (ny * hL + 31) / 32;
-        };
-        if (d.nslots % 2 == 0) {
-          int rp2 = 1;
-          while (rp2 * 2 < d.nslots) rp2 <<= 1;
-          const int p2 = (d.lattice == SA_LATTICE_3D) ? passes_for(rp2) : passes_for(rp2) * rp2 / d.P;
-          if (p2 >= 12 || d.lattice != SA_LATTICE_3D) {
-            g.SL = 2;
-            g.RP = rp2;
-          }
-        }
-        const int passes = passes_for(g.RP);
-        int warps = std::min(passes, kResMaxWarps);
-        const int rounds = (passes + warps - 1) / warps;
-        warps = std::max(4, (passes + rounds - 1) / rounds);
-        g.threads = warps * 32;
-      }
-      b->groups.push_back(g);
+  // energy histograms: PT instances only, when requested before finalize
+  b->hist_count = 0;
+  for (InstDesc& d : b->inst) {
+    d.hist_off = -1;
+    if (b->hstride > 0 && d.ladder >= 0) {
+      d.hist_off = b->hist_count;
+      b->hist_count += (int64_t)d.nslots * (d.nbonds + 1);
     }
-    sa_batch::Group& g = b->groups.back();
-    g.count += 1;
-    g.smem = std::max(g.smem, smem);
   }
+  if (b->hist_count) {
+    for (const auto& gcheck : b->inst)
+      if (gcheck.hist_off >= 0 && b->force_global)
+        return fail(SA_ERR_UNSUPPORTED, "energy histograms need the resident kernel");
+    SA_CUDA_TRY(cudaMalloc(&b->d_hist, b->hist_count * sizeof(int32_t)));
+    SA_CUDA_TRY(cudaMemsetAsync(b->d_hist, 0, b->hist_count * sizeof(int32_t), b->stream));
+  }
+  std::vector<int32_t> order = build_groups(b);
   const size_t ni = b->inst.size();
   SA_CUDA_TRY(cudaMalloc(&b->d_inst, ni * sizeof(InstDesc)));
   SA_CUDA_TRY(cudaMalloc(&b->d_state, ni * sizeof(InstState)));
@@ -1165,6 +1222,29 @@ int sa_batch_finalize(sa_batch_t b) {
 int sa_batch_set_exchange_interval(sa_batch_t b, int k) {
   if (!b || k < 1) return fail(SA_ERR_INVALID, "interval must be >= 1");
   b->xinterval = k;
+  return SA_OK;
+}
+
+int sa_batch_set_histograms(sa_batch_t b, int stride) {
+  if (!b || stride < 0) return fail(SA_ERR_INVALID, "stride must be >= 0");
+  if (b->finalized) return fail(SA_ERR_INVALID, "enable histograms before finalize");
+  b->hstride = stride;
+  return SA_OK;
+}
+
+int sa_batch_histogram(sa_batch_t b, int id, int slot, int32_t* out, long cap, long* nbins) {
+  if (!b || !nbins) return fail(SA_ERR_INVALID, "null argument");
+  if (!b->finalized) return fail(SA_ERR_INVALID, "finalize the batch first");
+  if (id < 0 || id >= (int)b->inst.size()) return fail(SA_ERR_INVALID, "instance id out of range");
+  const InstDesc& d = b->inst[id];
+  if (d.hist_off < 0) return fail(SA_ERR_INVALID, "no histograms for this instance");
+  if (slot < 0 || slot >= d.nslots) return fail(SA_ERR_INVALID, "bad slot");
+  *nbins = (long)(d.nbonds + 1);
+  if (!out) return SA_OK;
+  if (cap < *nbins) return fail(SA_ERR_BUFFER, "histogram buffer too small");
+  SA_CUDA_TRY(cudaMemcpyAsync(out, b->d_hist + d.hist_off + (long)slot * (d.nbonds + 1),
+                              (size_t)(d.nbonds + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, b->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
   return SA_OK;
 }
 
@@ -1435,6 +1515,383 @@ int sa_batch_sweeps_done(sa_batch_t b, int id, long* sweeps_done) {
   SA_CUDA_TRY(cudaMemcpyAsync(&s, b->d_state + id, sizeof s, cudaMemcpyDeviceToHost, b->stream));
   SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
   *sweeps_done = (long)s.sweeps;
+  return SA_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Serving: continuous batching of anneal requests.
+//
+// A serving object owns device pools sized from a memory budget: one word pool
+// for spins and couplings (first-fit free list), a threshold pool (one entry
+// per schedule step) and a table of per-request states. A request is admitted
+// only when all three have room; it is initialised on the device (couplings
+// from seed_J, spins from seed, like a batch instance) and stays resident until
+// it has run its whole schedule. Every round rebuilds the instance table from
+// the active requests, groups it by shape and launches the same kernels as
+// sa_batch_run for a chunk of sweeps; requests that arrive meanwhile join at
+// the next round. Each request's random stream is keyed by its own seed, so
+// its result does not depend on what else runs beside it.
+// ===========================================================================
+namespace {
+
+struct FreeList {
+  std::map<int64_t, int64_t> free;  // offset -> length
+  int64_t cap = 0;
+  void init(int64_t n) {
+    cap = n;
+    free.clear();
+    if (n > 0) free[0] = n;
+  }
+  int64_t alloc(int64_t n) {
+    for (auto it = free.begin(); it != free.end(); ++it) {
+      if (it->second >= n) {
+        const int64_t off = it->first, len = it->second;
+        free.erase(it);
+        if (len > n) free[off + n] = len - n;
+        return off;
+      }
+    }
+    return -1;
+  }
+  void release(int64_t off, int64_t n) {
+    auto it = free.emplace(off, n).first;
+    auto nx = std::next(it);
+    if (nx != free.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free.erase(nx);
+    }
+    if (it != free.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free.erase(it);
+      }
+    }
+  }
+};
+
+struct ServeReq {
+  InstDesc d;
+  int64_t words;     // spin + coupling words held
+  int64_t thr_n;     // threshold entries held
+  int64_t sweeps;    // host mirror of the sweeps done
+  bool fresh;        // needs device initialisation
+  uint64_t seed_J;
+};
+
+}  // namespace
+
+struct sa_serve {
+  sa_batch b;  // kernel context: pools as d_spins/d_J/d_thr/d_state
+  FreeList words, thr;
+  std::vector<int> free_states;
+  std::map<int64_t, ServeReq> active;  // by request id
+  std::vector<int64_t> finished;
+  int64_t next_id = 1;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;
+  std::vector<BThr> thr_stage;
+  size_t budget = 0;
+};
+
+extern "C" {
+
+int sa_serve_create(size_t budget_bytes, int max_requests, sa_serve_t* out) {
+  if (!out || max_requests < 1 || budget_bytes < (1u << 20)) return fail(SA_ERR_INVALID, "bad serving parameters");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SA_ERR_NO_DEVICE, "no CUDA device available");
+  sa_serve* s = new sa_serve();
+  sa_batch& b = s->b;
+  cudaGetDevice(&b.device);
+  auto bail = [&](cudaError_t e, const char* w) {
+    int st = cuda_fail(e, w);
+    sa_serve_destroy(s);
+    return st;
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&b.own_stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+  b.stream = b.own_stream;
+  // budget: 1/16 for thresholds (64 B each), states (~1.1 KB each), the rest words
+  const size_t state_bytes = (size_t)max_requests * sizeof(InstState);
+  const size_t thr_bytes = budget_bytes / 16;
+  if (state_bytes + thr_bytes >= budget_bytes) {
+    delete s;
+    return fail(SA_ERR_BUDGET, "budget too small for the request table");
+  }
+  const int64_t nwords = (int64_t)((budget_bytes - state_bytes - thr_bytes) / sizeof(word_t));
+  const int64_t nthr = (int64_t)(thr_bytes / sizeof(BThr));
+  if ((e = cudaMalloc(&b.d_spins, nwords * sizeof(word_t))) != cudaSuccess) return bail(e, "word pool");
+  b.d_J = b.d_spins;
+  if ((e = cudaMalloc(&b.d_thr, nthr * sizeof(BThr))) != cudaSuccess) return bail(e, "threshold pool");
+  if ((e = cudaMalloc(&b.d_state, state_bytes)) != cudaSuccess) return bail(e, "state table");
+  if ((e = cudaMalloc(&b.d_acc, sizeof(int64_t))) != cudaSuccess) return bail(e, "acc");
+  if ((e = cudaMalloc(&b.d_att, sizeof(int64_t))) != cudaSuccess) return bail(e, "att");
+  s->words.init(nwords);
+  s->thr.init(nthr);
+  for (int i = max_requests - 1; i >= 0; --i) s->free_states.push_back(i);
+  for (int i = 0; i < 16; ++i) {
+    cudaStream_t st;
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+    s->streams.push_back(st);
+  }
+  if ((e = cudaEventCreateWithFlags(&b.fork, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
+  b.finalized = true;
+  s->budget = budget_bytes;
+  *out = s;
+  return SA_OK;
+}
+
+int sa_serve_destroy(sa_serve_t s) {
+  if (!s) return SA_OK;
+  sa_batch& b = s->b;
+  if (b.stream) cudaStreamSynchronize(b.stream);
+  for (auto st : s->streams) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  for (auto ev : s->events) cudaEventDestroy(ev);
+  if (b.fork) cudaEventDestroy(b.fork);
+  b.fork = nullptr;
+  cudaFree(b.d_spins);
+  cudaFree(b.d_thr);
+  cudaFree(b.d_state);
+  cudaFree(b.d_acc);
+  cudaFree(b.d_att);
+  cudaFree(b.d_inst);
+  cudaFree(b.d_order);
+  cudaFree(b.d_work);
+  b.d_spins = b.d_J = nullptr;
+  b.d_thr = nullptr;
+  b.d_state = nullptr;
+  b.d_acc = b.d_att = nullptr;
+  b.d_inst = nullptr;
+  b.d_order = nullptr;
+  b.d_work = nullptr;
+  b.groups.clear();  // the group streams belong to s->streams
+  if (b.own_stream) cudaStreamDestroy(b.own_stream);
+  b.own_stream = nullptr;
+  delete s;
+  return SA_OK;
+}
+
+int sa_serve_set_stream(sa_serve_t s, void* stream) {
+  if (!s) return fail(SA_ERR_INVALID, "null server");
+  s->b.stream = stream ? (cudaStream_t)stream : s->b.own_stream;
+  return SA_OK;
+}
+
+// Admits an anneal request if the pools have room now (SA_ERR_BUDGET if not).
+int sa_serve_submit(sa_serve_t s, int lattice, int L, uint64_t seed_J, uint64_t seed, const double* T, int nsteps,
+                    int sweeps_per_step, int64_t* id) {
+  if (!s || !T || !id) return fail(SA_ERR_INVALID, "null argument");
+  if (lattice < 0 || lattice > 2) return fail(SA_ERR_INVALID, "unknown lattice kind");
+  if (L < 2) return fail(SA_ERR_INVALID, "L must be >= 2");
+  if (L & 1) return fail(SA_ERR_ODD_L, "L must be even");
+  if (nsteps < 1 || sweeps_per_step < 1) return fail(SA_ERR_INVALID, "empty schedule");
+  InstDesc d;
+  memset(&d, 0, sizeof d);
+  const int dim = lattice_dim(lattice);
+  d.lattice = lattice;
+  d.L = L;
+  d.N = (dim == 3) ? (int64_t)L * L * L : (int64_t)L * L;
+  if (d.N > kBatchMaxN) return fail(SA_ERR_UNSUPPORTED, "request too large");
+  d.half = d.N / 2;
+  d.nbonds = dim * d.N - (lattice == SA_LATTICE_2D_OPEN_X ? L : 0);
+  d.nslots = 1;
+  d.P = 1;
+  d.ladder = -1;
+  d.sched = 0;
+  d.seed = seed;
+  d.sweeps_per_step = sweeps_per_step;
+  d.thr_count = nsteps;
+  d.sweep_limit = (int64_t)nsteps * sweeps_per_step;
+  d.hist_off = -1;
+  std::vector<BThr> thr(nsteps);
+  for (int k = 0; k < nsteps; ++k) {
+    if (!(T[k] > 0)) return fail(SA_ERR_INVALID, "temperatures must be > 0");
+    thr[k] = to_bthr(lattice, T[k]);
+  }
+  if (s->free_states.empty()) return fail(SA_ERR_BUDGET, "request table full");
+  const int64_t words = d.N + dim * d.N;
+  const int64_t woff = s->words.alloc(words);
+  if (woff < 0) return fail(SA_ERR_BUDGET, "memory budget full");
+  const int64_t toff = s->thr.alloc(nsteps);
+  if (toff < 0) {
+    s->words.release(woff, words);
+    return fail(SA_ERR_BUDGET, "threshold pool full");
+  }
+  const int st = s->free_states.back();
+  s->free_states.pop_back();
+  d.spin_off = woff;
+  d.J_off = woff + d.N;
+  d.thr_off = toff;
+  d.state_idx = st;
+  SA_CUDA_TRY(cudaMemcpyAsync(s->b.d_thr + toff, thr.data(), nsteps * sizeof(BThr), cudaMemcpyHostToDevice,
+                              s->b.stream));
+  SA_CUDA_TRY(cudaMemsetAsync(s->b.d_state + st, 0, sizeof(InstState), s->b.stream));
+  ServeReq r;
+  r.d = d;
+  r.words = words;
+  r.thr_n = nsteps;
+  r.sweeps = 0;
+  r.fresh = true;
+  r.seed_J = seed_J;
+  *id = s->next_id++;
+  s->active.emplace(*id, r);
+  SA_CUDA_TRY(cudaStreamSynchronize(s->b.stream));  // thresholds staged from pageable memory
+  return SA_OK;
+}
+
+// One round: every active request advances by up to nsweeps sweeps.
+int sa_serve_run(sa_serve_t s, long nsweeps) {
+  if (!s || nsweeps < 1) return fail(SA_ERR_INVALID, "bad arguments");
+  sa_batch& b = s->b;
+  // device initialisation of the requests admitted since the last round
+  std::vector<InstDesc> fresh;
+  std::vector<uint64_t> fresh_seedJ;
+  int64_t maxN = 0;
+  for (auto& kv : s->active)
+    if (kv.second.fresh) {
+      fresh.push_back(kv.second.d);
+      fresh_seedJ.push_back(kv.second.seed_J);
+      maxN = std::max<int64_t>(maxN, kv.second.d.N);
+      kv.second.fresh = false;
+    }
+  b.inst.clear();
+  for (auto& kv : s->active)
+    if (kv.second.sweeps < kv.second.d.sweep_limit) b.inst.push_back(kv.second.d);
+  const size_t ni = b.inst.size();
+  const size_t need = std::max(ni, fresh.size());
+  if (need > b.inst_cap) {
+    SA_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    cudaFree(b.d_inst);
+    cudaFree(b.d_order);
+    cudaFree(b.d_seedJ);
+    b.inst_cap = std::max<size_t>(need, 2 * b.inst_cap);
+    SA_CUDA_TRY(cudaMalloc(&b.d_inst, b.inst_cap * sizeof(InstDesc)));
+    SA_CUDA_TRY(cudaMalloc(&b.d_order, b.inst_cap * sizeof(int32_t)));
+    SA_CUDA_TRY(cudaMalloc(&b.d_seedJ, b.inst_cap * sizeof(uint64_t)));
+  }
+  if (!fresh.empty()) {
+    SA_CUDA_TRY(cudaMemcpyAsync(b.d_inst, fresh.data(), fresh.size() * sizeof(InstDesc), cudaMemcpyHostToDevice,
+                                b.stream));
+    SA_CUDA_TRY(cudaMemcpyAsync(b.d_seedJ, fresh_seedJ.data(), fresh.size() * sizeof(uint64_t),
+                                cudaMemcpyHostToDevice, b.stream));
+    dim3 g((unsigned)((maxN + 255) / 256), (unsigned)fresh.size());
+    k_batch_init<<<g, 256, 0, b.stream>>>(b.d_inst, b.d_seedJ, b.d_spins, b.d_J);
+    SA_CUDA_TRY(cudaGetLastError());
+  }
+  if (ni == 0) return SA_OK;
+  std::vector<int32_t> order = build_groups(&b);
+  if (b.groups.size() > b.work_cap) {
+    SA_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    cudaFree(b.d_work);
+    b.work_cap = std::max<size_t>(b.groups.size(), 2 * b.work_cap);
+    SA_CUDA_TRY(cudaMalloc(&b.d_work, b.work_cap * sizeof(int32_t)));
+  }
+  while (s->events.size() < b.groups.size()) {
+    cudaEvent_t ev;
+    SA_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    s->events.push_back(ev);
+  }
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.device);
+  for (size_t gi = 0; gi < b.groups.size(); ++gi) {
+    sa_batch::Group& g = b.groups[gi];
+    g.stream = s->streams[gi % s->streams.size()];
+    g.done = s->events[gi];
+    if (g.resident) {
+      int mc = 0;
+      int st = dispatch(&b, g, (int)gi, 0, 1, &mc);  // kernel attributes (cheap after the first time)
+      if (st) return st;
+    } else {
+      g.grid = (int)std::min<int64_t>((int64_t)sms, (int64_t)g.count);
+    }
+  }
+  // the pageable uploads below complete before the call returns
+  SA_CUDA_TRY(cudaMemcpyAsync(b.d_inst, b.inst.data(), ni * sizeof(InstDesc), cudaMemcpyHostToDevice, b.stream));
+  SA_CUDA_TRY(cudaMemcpyAsync(b.d_order, order.data(), ni * sizeof(int32_t), cudaMemcpyHostToDevice, b.stream));
+  SA_CUDA_TRY(cudaMemsetAsync(b.d_work, 0, b.groups.size() * sizeof(int32_t), b.stream));
+  SA_CUDA_TRY(cudaEventRecord(b.fork, b.stream));
+  for (size_t gi = 0; gi < b.groups.size(); ++gi) {
+    SA_CUDA_TRY(cudaStreamWaitEvent(b.groups[gi].stream, b.fork, 0));
+    int st = dispatch(&b, b.groups[gi], (int)gi, nsweeps, 0, nullptr);
+    if (st) return st;
+    SA_CUDA_TRY(cudaEventRecord(b.groups[gi].done, b.groups[gi].stream));
+  }
+  for (size_t gi = 0; gi < b.groups.size(); ++gi) SA_CUDA_TRY(cudaStreamWaitEvent(b.stream, b.groups[gi].done, 0));
+  SA_CUDA_TRY(cudaGetLastError());
+  // host mirror of the progress; finished requests are reported by poll
+  for (auto& kv : s->active) {
+    ServeReq& r = kv.second;
+    if (r.sweeps >= r.d.sweep_limit) continue;
+    r.sweeps = std::min<int64_t>(r.d.sweep_limit, r.sweeps + nsweeps);
+    if (r.sweeps >= r.d.sweep_limit) s->finished.push_back(kv.first);
+  }
+  return SA_OK;
+}
+
+int sa_serve_sync(sa_serve_t s) {
+  if (!s) return fail(SA_ERR_INVALID, "null server");
+  SA_CUDA_TRY(cudaStreamSynchronize(s->b.stream));
+  return SA_OK;
+}
+
+// Requests that completed their schedule (their results are final once the
+// rounds that finished them have completed: sync first).
+int sa_serve_poll(sa_serve_t s, int64_t* ids, int cap, int* n) {
+  if (!s || !n) return fail(SA_ERR_INVALID, "null argument");
+  const int k = (int)std::min<size_t>((size_t)std::max(cap, 0), s->finished.size());
+  for (int i = 0; i < k; ++i) ids[i] = s->finished[i];
+  s->finished.erase(s->finished.begin(), s->finished.begin() + k);
+  *n = k;
+  return SA_OK;
+}
+
+// Result of a finished request: running max of -H per replica (int64[64]),
+// the last measured -H per replica (may be NULL) and the final spins in
+// row-major order (may be NULL); then frees everything it held.
+int sa_serve_result(sa_serve_t s, int64_t id, int64_t* Emax, int64_t* Elast, uint64_t* spins) {
+  if (!s) return fail(SA_ERR_INVALID, "null server");
+  auto it = s->active.find(id);
+  if (it == s->active.end()) return fail(SA_ERR_INVALID, "unknown request id");
+  ServeReq& r = it->second;
+  if (r.sweeps < r.d.sweep_limit) return fail(SA_ERR_INVALID, "request has not finished");
+  sa_batch& b = s->b;
+  InstState st;
+  SA_CUDA_TRY(cudaMemcpyAsync(&st, b.d_state + r.d.state_idx, sizeof st, cudaMemcpyDeviceToHost, b.stream));
+  if (spins) {
+    std::vector<word_t> raw(r.d.N);
+    SA_CUDA_TRY(cudaMemcpyAsync(raw.data(), b.d_spins + r.d.spin_off, r.d.N * sizeof(word_t), cudaMemcpyDeviceToHost,
+                                b.stream));
+    SA_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    const long L = r.d.L, hL = L / 2;
+    for (long i = 0; i < r.d.N; ++i) {
+      const long row = i / L;
+      const int x = (int)(i - row * L), y = (int)(row % L), c = (x + y) & 1;
+      spins[i] = raw[(long)c * r.d.half + row * hL + (x >> 1)];
+    }
+  }
+  SA_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  if (Emax) memcpy(Emax, st.emax, sizeof st.emax);
+  if (Elast) memcpy(Elast, st.elast, sizeof st.elast);
+  s->words.release(r.d.spin_off, r.words);
+  s->thr.release(r.d.thr_off, r.thr_n);
+  s->free_states.push_back((int)r.d.state_idx);
+  s->active.erase(it);
+  return SA_OK;
+}
+
+int sa_serve_active(sa_serve_t s, int* n, long long* free_words) {
+  if (!s) return fail(SA_ERR_INVALID, "null server");
+  if (n) *n = (int)s->active.size();
+  if (free_words) {
+    long long f = 0;
+    for (auto& kv : s->words.free) f += kv.second;
+    *free_words = f;
+  }
   return SA_OK;
 }
 

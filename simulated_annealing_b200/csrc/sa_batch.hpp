@@ -29,6 +29,8 @@ struct InstDesc {
   int64_t thr_off;                 // index of slot 0 / step 0 in the threshold pool
   int64_t dec_off, dec_count;      // ladder's exchange table
   int64_t pair_off;                // acceptance counters (nslots-1 pairs)
+  int64_t hist_off;                // energy histograms: nslots x (nbonds+1) bins, -1 = none
+  int64_t state_idx;               // index of this instance's InstState
   uint64_t seed;
   int64_t sweep_limit;             // anneal: steps * sweeps_per_step; PT: -1
 };
@@ -60,6 +62,8 @@ struct BatchParams {
   int64_t nsweeps;         // requested sweeps this launch
   int32_t xinterval;       // sweeps between exchanges
   int32_t mstride;         // anneal measure stride (0 = never)
+  int32_t* hist;           // energy histograms (bin (E+nbonds)/2), or null
+  int32_t hstride;         // histogram every hstride sweeps
 };
 
 }  // namespace sa

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <random>
 
 #include "sa_b200.h"
 
@@ -128,3 +129,37 @@ void pt_accept_interval(double dB, double r, int64_t span, int64_t* lo, int64_t*
 }  // namespace sa
 
 extern "C" const char* sa_last_error(void) { return sa::g_last_error.c_str(); }
+
+// The exchange sequence of parallel_tempering<> (src/parallel_tempering.hpp:
+// 193-198, 251-253): std::mt19937 gen(123); per step i = uni_int(gen) from
+// uniform_int_distribution<int>(0, n-2), then r = uni_double(gen) from
+// uniform_real_distribution<double>(0, 1) -- libstdc++'s own generators.
+extern "C" int sa_pt_sequence(int n, long skip, long count, int32_t* pair, double* r) {
+  if (n < 2 || skip < 0 || count < 0 || (count > 0 && (!pair || !r)))
+    return sa::fail(SA_ERR_INVALID, "bad arguments to sa_pt_sequence");
+  std::mt19937 gen(123);
+  std::uniform_int_distribution<int> uni_int(0, n - 2);
+  std::uniform_real_distribution<double> uni_double(0., 1.);
+  for (long k = 0; k < skip + count; ++k) {
+    const int i = uni_int(gen);
+    const double u = uni_double(gen);
+    if (k >= skip) {
+      pair[k - skip] = i;
+      r[k - skip] = u;
+    }
+  }
+  return SA_OK;
+}
+
+// The reference's per-replica exchange test (src/parallel_tempering.hpp:
+// 141-162) for one pair: mask bit j set iff dE*dB > 0 || r < exp(dB*dE) with
+// dE = -(Ei[j] - Ej[j]) as float and dB = 1/Ti - 1/Tj.
+extern "C" uint64_t sa_pt_mask(const float* Ei, const float* Ej, double Ti, double Tj, double r) {
+  const double dB = (1. / Ti - 1. / Tj);
+  uint64_t mask = 0;
+  for (int j = 0; j < 64; ++j) {
+    const float dE = -(Ei[j] - Ej[j]);
+    if (sa::pt_accept(dE, dB, r)) mask |= 1ULL << j;
+  }
+  return mask;
+}

@@ -177,3 +177,45 @@ def test_resident_groups(sab):
         b.add_instance(O.LAT_3D, L, ladder=lad, seed_J=L, seed=L)
     b.finalize()
     assert 1 <= b.launches_per_run() <= 5
+
+
+@pytest.mark.parametrize("lat,L,nslots", [(O.LAT_3D, 6, 8), (O.LAT_2D, 10, 5)])
+def test_energy_histograms_and_decisions(sab, lat, L, nslots):
+    """C3-style run: exchange every sweep, per-slot energy histograms (taken
+    before the exchange, like the reference's E[]), acceptance and every
+    decision, against the oracle's parallel_tempering<> restatement."""
+    from simulated_annealing_b200.batch import Batch
+    T = list(np.geomspace(0.5, 2.0, nslots))
+    sweeps = 40
+    b = Batch()
+    lad = b.add_ladder(T)
+    b.add_instance(lat, L, ladder=lad, seed_J=4, seed=4)
+    b.set_histograms(1)
+    b.finalize()
+    b.record_exchanges(sweeps)
+    b.run(15)
+    b.run(sweeps - 15)
+    b.sync()
+    systems = [O.OracleSystem(lat, L, mode=O.MODE_PHILOX) for _ in T]
+    for s in systems:
+        s.set_seed(4)
+        s.init_J()
+        s.set_seed(4)
+        s.init_rand()
+    pt = O.OraclePT(systems, T, 1)
+    N = L ** 3 if lat == O.LAT_3D else L * L
+    nbonds = (3 if lat == O.LAT_3D else 2) * N
+    hist = np.zeros((nslots, nbonds + 1), dtype=np.int64)
+    steps = []
+    for _ in range(sweeps):
+        steps.append(pt.step(0))
+        E = pt.energies().astype(np.int64)
+        for s in range(nslots):
+            np.add.at(hist[s], (E[s] + nbonds) // 2, 1)
+    pairs, masks = b.exchanges(0)
+    assert pairs.tolist() == [p for p, _, _ in steps]
+    assert [int(m) for m in masks] == [m for _, m, _ in steps]
+    for s in range(nslots):
+        assert np.array_equal(b.histogram(0, s), hist[s]), s
+    acc, att = b.acceptance(0)
+    assert np.allclose(acc / np.maximum(att, 1) / 64.0, pt.acceptance(), rtol=0, atol=1e-12)
