@@ -387,8 +387,15 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
   x.hL = d.L >> 1;
   x.ns = d.nslots;
   x.zc = (LAT == SA_LATTICE_3D) ? d.L : 1;
-  x.ny = d.L / C;
-  x.y0 = q * x.ny;
+  {
+    // rows split as evenly as L allows: the first L%C CTAs take one extra
+    const int base = d.L / C, rem = d.L % C;
+    auto rows_of = [&](int r) { return base + (r < rem ? 1 : 0); };
+    x.ny = rows_of(q);
+    x.y0 = q * base + min(q, rem);
+    x.nyN = rows_of((q + C - 1) % C);
+    x.nyS = rows_of((q + 1) % C);
+  }
   x.rowW = x.hL * x.ns;
   x.half = (int)d.half;
   x.seed = d.seed;
@@ -443,7 +450,10 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
       }
     }
     for (int c = 0; c < 2; ++c) {
-      if (d3) rhalf_3d<P, SL>(x, c, draw + c, th);
+      if (d3) {
+        if (P == 1 && SL == 1 && x.L > 4) rhalf_3d1<4>(x, c, draw + c, th[0]);
+        else rhalf_3d<P, SL>(x, c, draw + c, th);
+      }
       else rhalf_2d<P, SL, open>(x, c, draw + c, th, tb);
       sync_all();
     }
@@ -552,15 +562,11 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
 // Set-up kernels: couplings from seed_J (draws 0..2*dim-1, src/random.cu:25-35)
 // and spins (engine init, epoch 0) copied into every slot.
 // ---------------------------------------------------------------------------
-__global__ void k_batch_init(const InstDesc* inst, const uint64_t* seed_J, word_t* spins, word_t* J) {
-  const InstDesc d = inst[blockIdx.y];
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.N) return;
+__device__ void init_site(const InstDesc& d, uint64_t sj, long i, word_t* spins, word_t* J) {
   const int L = d.L, hL = L >> 1, dim = d.lattice == SA_LATTICE_3D ? 3 : 2;
   const long r = i / L;
   const int x = (int)(i - r * L), y = (int)(r % L), c = (x + y) & 1;
   const long rem = r * hL + (x >> 1);
-  const uint64_t sj = seed_J[blockIdx.y];
   uint4x b0 = philox10(0, 0, (uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)sj, (uint32_t)(sj >> 32));
   uint4x b1 = philox10(1, 0, (uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)sj, (uint32_t)(sj >> 32));
   const uint32_t dr[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
@@ -572,6 +578,14 @@ __global__ void k_batch_init(const InstDesc* inst, const uint64_t* seed_J, word_
   const word_t w = (word_t)s.x | ((word_t)s.y << 32);
   word_t* Sd = spins + d.spin_off + ((long)c * d.half + rem) * d.nslots;
   for (int q = 0; q < d.nslots; ++q) Sd[q] = w;
+}
+
+__global__ void k_batch_init(const InstDesc* inst, const uint64_t* seed_J, int ninst, word_t* spins, word_t* J) {
+  for (int id = blockIdx.y; id < ninst; id += gridDim.y) {
+    const InstDesc d = inst[id];
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < d.N) init_site(d, seed_J[id], i, spins, J);
+  }
 }
 
 __global__ void k_batch_gather(const word_t* spins, const InstDesc* inst, int id, int slot, word_t* out) {
@@ -698,12 +712,21 @@ constexpr size_t kResSmemBudget = 232448 - 8192;
 // Smallest cluster size C dividing L whose per-CTA share of the instance's
 // spins fits the budget; 0 if none does (the instance then runs in the
 // global-memory kernel).
+// Shared-memory bytes of the largest CTA when an instance's y-rows are split
+// over C CTAs (ceil(L/C) rows of every z-plane and both colours).
+static size_t resident_bytes(const InstDesc& d, int C) {
+  const int zc = (d.lattice == SA_LATTICE_3D) ? d.L : 1;
+  const int ny = (d.L + C - 1) / C;
+  return (size_t)2 * zc * ny * (d.L / 2) * d.nslots * sizeof(word_t);
+}
+
+// Smallest cluster whose CTAs hold their share of the instance in shared
+// memory; 0 = too large (the instance streams from global memory instead).
 static int choose_cluster(const InstDesc& d) {
   static const int cands[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
-  const size_t bytes = (size_t)d.N * d.nslots * sizeof(word_t);
   for (int C : cands) {
-    if (C > d.L || d.L % C) continue;
-    if (bytes / C <= kResSmemBudget) return C;
+    if (C > d.L) break;
+    if (resident_bytes(d, C) <= kResSmemBudget) return C;
   }
   return 0;
 }
@@ -768,7 +791,7 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
   for (size_t i = 0; i < order.size(); ++i) {
     const InstDesc& d = b->inst[order[i]];
     const int C = b->cluster_of[order[i]];
-    const size_t smem = C ? (size_t)d.N * d.nslots * sizeof(word_t) / C : 0;
+    const size_t smem = C ? resident_bytes(d, C) : 0;
     const bool same = !b->groups.empty() && b->groups.back().resident == (C != 0) && b->groups.back().P == d.P &&
                       b->groups.back().C == C &&
                       (C == 0 || (b->groups.back().lattice == d.lattice && b->groups.back().L == d.L));
@@ -788,7 +811,7 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
         // takes tiles of 32 sites (RP sub-steps of 32/RP sites each). Two slots
         // per lane (16-byte accesses, shared addressing and couplings) when the
         // slot count is even and there is still work for >= 12 warps.
-        const int ny = d.L / C, hL = d.L / 2;
+        const int ny = (d.L + C - 1) / C, hL = d.L / 2;
         auto passes_for = [&](int rp) {
           return (d.lattice == SA_LATTICE_3D) ? (ny * hL + (32 / rp) - 1) / (32 / rp) : (ny * hL + 31) / 32;
         };
@@ -1190,8 +1213,8 @@ int sa_batch_finalize(sa_batch_t b) {
   uint64_t* d_seedJ = nullptr;
   SA_CUDA_TRY(cudaMalloc(&d_seedJ, ni * sizeof(uint64_t)));
   SA_CUDA_TRY(cudaMemcpyAsync(d_seedJ, b->seed_J.data(), ni * sizeof(uint64_t), cudaMemcpyHostToDevice, b->stream));
-  dim3 g((unsigned)((maxN + 255) / 256), (unsigned)ni);
-  k_batch_init<<<g, 256, 0, b->stream>>>(b->d_inst, d_seedJ, b->d_spins, b->d_J);
+  dim3 g((unsigned)((maxN + 255) / 256), (unsigned)std::min<size_t>(ni, 65535));
+  k_batch_init<<<g, 256, 0, b->stream>>>(b->d_inst, d_seedJ, (int)ni, b->d_spins, b->d_J);
   SA_CUDA_TRY(cudaGetLastError());
   SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
   cudaFree(d_seedJ);
@@ -1779,8 +1802,8 @@ int sa_serve_run(sa_serve_t s, long nsweeps) {
                                 b.stream));
     SA_CUDA_TRY(cudaMemcpyAsync(b.d_seedJ, fresh_seedJ.data(), fresh.size() * sizeof(uint64_t),
                                 cudaMemcpyHostToDevice, b.stream));
-    dim3 g((unsigned)((maxN + 255) / 256), (unsigned)fresh.size());
-    k_batch_init<<<g, 256, 0, b.stream>>>(b.d_inst, b.d_seedJ, b.d_spins, b.d_J);
+    dim3 g((unsigned)((maxN + 255) / 256), (unsigned)std::min<size_t>(fresh.size(), 65535));
+    k_batch_init<<<g, 256, 0, b.stream>>>(b.d_inst, b.d_seedJ, (int)fresh.size(), b.d_spins, b.d_J);
     SA_CUDA_TRY(cudaGetLastError());
   }
   if (ni == 0) return SA_OK;

@@ -1,11 +1,12 @@
 // sa_resident.cuh -- the shared-memory-resident batched kernel.
 //
 // One instance (all its slots) is held in the shared memory of a thread-block
-// cluster of C CTAs for a whole launch: CTA q owns the y-rows
-// [q*L/C, (q+1)*L/C) of every z-plane and both colours, layout
+// cluster of C CTAs for a whole launch: CTA q owns ny_q consecutive y-rows
+// starting at y0_q (ny_q = L/C, plus one for the first L%C CTAs) of every
+// z-plane and both colours, layout
 //   [colour][z][y_local][k][slot]            (k = x/2, slot innermost)
 // and reads the two halo rows it needs (y0-1, y0+ny) from the neighbouring
-// CTAs' shared memory over DSMEM. Couplings stay in global memory (L2) and
+// CTAs' shared memory over DSMEM (whose layouts use their own row counts). Couplings stay in global memory (L2) and
 // are shared by the slots of a site. Between half-sweeps the cluster
 // synchronises; the replica exchange sums per-CTA energy partials over DSMEM,
 // so every CTA reaches the same decision and swaps its own rows.
@@ -33,6 +34,7 @@ struct ResCtx {
   const word_t* J;      // instance couplings [axis][colour][row][k] (global)
   uint64_t seed;
   int L, hL, ny, y0, ns, zc;  // zc: z-planes (L in 3D, 1 in 2D)
+  int nyN, nyS;               // rows held by the CTAs owning y0-1 and y0+ny
   int half;                   // sites per colour of the instance (global J stride)
   int rowW;                   // words per local row: hL*ns
   uint32_t magic;             // floor(2^32/hL)+1, for division by hL
@@ -49,6 +51,14 @@ __device__ __forceinline__ int div_hl(int t, const ResCtx& x) {
 // local word offset of (colour, z, y_local) row start
 __device__ __forceinline__ int lrow(const ResCtx& x, int c, int z, int yl) {
   return ((c * x.zc + z) * x.ny + yl) * x.rowW;
+}
+
+// the halo rows: last row of the north neighbour, first row of the south one
+__device__ __forceinline__ int lrow_n(const ResCtx& x, int c, int z) {
+  return ((c * x.zc + z) * x.nyN + x.nyN - 1) * x.rowW;
+}
+__device__ __forceinline__ int lrow_s(const ResCtx& x, int c, int z) {
+  return ((c * x.zc + z) * x.nyS) * x.rowW;
 }
 
 // SL consecutive slot words of one site (SL = 2: one 16-byte access).
@@ -115,8 +125,8 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
         x_neighbours(k, par, hL, kw, ke);
         const int own = lrow(x, c, 0, yl) + k * ns + slot;
         const int orow = lrow(x, oc, 0, yl);
-        const word_t* pn = (yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow(x, oc, 0, x.ny - 1);
-        const word_t* ps = (yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow(x, oc, 0, 0);
+        const word_t* pn = (yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow_n(x, oc, 0);
+        const word_t* ps = (yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow_s(x, oc, 0);
         const int ys = (y == L - 1) ? 0 : y + 1;
         const SlotWords<SL> si = ldw<SL>(x.sm + own);
         const SlotWords<SL> sw = ldw<SL>(x.sm + orow + kw * ns + slot);
@@ -180,8 +190,10 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
     int own = lrow(x, c, 0, yl) + k * ns + slot;
     int ow = lrow(x, oc, 0, yl) + kw * ns + slot;
     int oe = lrow(x, oc, 0, yl) + ke * ns + slot;
-    const word_t* pn = ((yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow(x, oc, 0, x.ny - 1)) + k * ns + slot;
-    const word_t* ps = ((yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow(x, oc, 0, 0)) + k * ns + slot;
+    const word_t* pn = ((yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow_n(x, oc, 0)) + k * ns + slot;
+    const word_t* ps = ((yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow_s(x, oc, 0)) + k * ns + slot;
+    const int zsn = (yl > 0) ? zs : x.nyN * x.rowW;       // z stride of the north row's owner
+    const int zss = (yl < x.ny - 1) ? zs : x.nyS * x.rowW;
     int jo = y * hL + k, je = y * hL + ke, js = ys * hL + k;
     SlotWords<SL> prev = {};
     if (valid) prev = ldw<SL>(x.sm + own + (L - 1) * zs);
@@ -224,11 +236,133 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         own += zs;
         ow += zs;
         oe += zs;
-        pn += zs;
-        ps += zs;
+        pn += zsn;
+        ps += zss;
         jo += zg;
         je += zg;
         js += zg;
+      }
+    }
+  }
+}
+
+// Satisfied-bond count of five bond words, bit-sliced (c2 c1 c0, 0..5).
+__device__ __forceinline__ void count5(word_t a, word_t b, word_t c, word_t d, word_t e, word_t& c0, word_t& c1,
+                                       word_t& c2) {
+  const word_t s1 = a ^ b ^ c;
+  const word_t k1 = (a & b) | (c & (a ^ b));
+  const word_t s2 = d ^ e;
+  const word_t k2 = d & e;
+  c0 = s1 ^ s2;
+  const word_t k3 = s1 & s2;
+  c1 = k1 ^ k2 ^ k3;
+  c2 = (k1 & k2) | (k3 & (k1 ^ k2));
+}
+
+// Replicas whose bit-sliced count (c2 c1 c0) is below the scalar t (bits
+// broadcast as masks m2 m1 m0).
+__device__ __forceinline__ word_t below(word_t c0, word_t c1, word_t c2, uint32_t m0, uint32_t m1, uint32_t m2) {
+  uint32_t r[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t a0 = (uint32_t)(c0 >> (32 * h)), a1 = (uint32_t)(c1 >> (32 * h));
+    const uint32_t a2 = (uint32_t)(c2 >> (32 * h));
+    const uint32_t g0 = a0 | ~m0;
+    const uint32_t g1 = (a1 & ~m1) | (~(a1 ^ m1) & g0);
+    r[h] = ~((a2 & ~m2) | (~(a2 ^ m2) & g1));
+  }
+  return (word_t)r[0] | ((word_t)r[1] << 32);
+}
+
+// Single-slot 3D half-sweep. Sites of one colour in one (x, y) column depend
+// on each other along z (the colour is (x+y)%2, so a site's z-1 neighbour has
+// its colour and is updated first). The walk is split in two phases per chunk
+// of Z planes: first every site's update is reduced to an affine map of the
+// one new value it depends on, the new z-1 spin x:
+//   new = A ^ (x & B),   A = s ^ f0,  B = f0 ^ f1,
+// with f0 / f1 the flips for x = 0 / 1 (the z-1 bond then counts g = J^s or
+// its complement, so f0 = g ? hi : lo and B = lo ^ hi, where lo / hi are the
+// flips with that bond unsatisfied / satisfied). The maps read only old
+// values, so their loads and Philox draws are independent; the chain then
+// applies Z maps at two logic operations each. The top plane's z+1
+// neighbour is the new z = 0 spin, known once the first chunk is applied
+// (requires L > Z).
+template <int Z>
+__device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw, const uint32_t* th) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int L = x.L, hL = x.hL;
+  const int cols = x.ny * hL;
+  const int oc = 1 - c;
+  const int zs = x.ny * x.rowW;  // local z stride (rowW == hL)
+  const int zg = L * hL;         // z stride of the coupling arrays
+  const word_t* Jxc = x.J + (long)(0 + c) * x.half;
+  const word_t* Jxo = x.J + (long)(1 - c) * x.half;
+  const word_t* Jyc = x.J + (long)(2 + c) * x.half;
+  const word_t* Jyo = x.J + (long)(3 - c) * x.half;
+  const word_t* Jzc = x.J + (long)(4 + c) * x.half;
+  for (int cb = warp * 32; cb < cols; cb += nwarps * 32) {
+    const int col = cb + lane;
+    if (col >= cols) break;  // the last columns; nothing below is warp-collective
+    const int yl = div_hl(col, x);
+    const int k = col - yl * hL;
+    const int y = x.y0 + yl;
+    const int par = (c + y) & 1, xx = 2 * k + par;
+    int kw, ke;
+    x_neighbours(k, par, hL, kw, ke);
+    const int ys = (y == L - 1) ? 0 : y + 1;
+    const word_t* own = x.sm + lrow(x, c, 0, yl) + k;
+    const word_t* pw = x.sm + lrow(x, oc, 0, yl) + kw;
+    const word_t* pe = x.sm + lrow(x, oc, 0, yl) + ke;
+    const word_t* pn = ((yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow_n(x, oc, 0)) + k;
+    const word_t* ps = ((yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow_s(x, oc, 0)) + k;
+    const int zsn = (yl > 0) ? zs : x.nyN * x.rowW;
+    const int zss = (yl < x.ny - 1) ? zs : x.nyS * x.rowW;
+    const int jo = y * hL + k, je = y * hL + ke, js = ys * hL + k;
+    const unsigned long long site0 = (unsigned long long)(xx + L * y), plane = (unsigned long long)L * L;
+    word_t* own_w = const_cast<word_t*>(own);
+    word_t prev = own[(L - 1) * zs];  // old top spin: the z-1 neighbour of z = 0
+    word_t first = 0;
+    for (int z0 = 0; z0 < L; z0 += Z) {
+      word_t A[Z], B[Z];
+#pragma unroll
+      for (int i = 0; i < Z; ++i) {
+        const int z = z0 + i;
+        A[i] = 0;
+        B[i] = 0;
+        if (z < L) {
+          const bool last = (z == L - 1);
+          const int zn = last ? 0 : z + 1;
+          const word_t si = own[z * zs];
+          const word_t sd = last ? first : own[zn * zs];
+          const word_t sw = pw[z * zs], se = pe[z * zs];
+          const word_t sn = pn[z * zsn], ss = ps[z * zss];
+          const word_t jw = __ldg(Jxc + jo + z * zg), jee = __ldg(Jxo + je + z * zg);
+          const word_t jn = __ldg(Jyc + jo + z * zg), jss = __ldg(Jyo + js + z * zg);
+          const word_t ju = __ldg(Jzc + jo + z * zg), jd = __ldg(Jzc + jo + zn * zg);
+          const uint32_t u = philox_draw(x.seed, site0 + plane * (unsigned)z, draw);
+          word_t c0, c1, c2;
+          count5(jw ^ sw ^ si, jee ^ se ^ si, jn ^ sn ^ si, jss ^ ss ^ si, jd ^ sd ^ si, c0, c1, c2);
+          uint32_t m0, m1, m2;
+          prefix_bits(u, th, m0, m1, m2);
+          // t - 1 (or 0): the prefix once the z-1 bond counts as satisfied
+          const uint32_t t = (m0 & 1u) | (m1 & 2u) | (m2 & 4u);
+          const uint32_t t1 = t ? t - 1 : 0;
+          const word_t lo = below(c0, c1, c2, m0, m1, m2);
+          const word_t hi = below(c0, c1, c2, (t1 & 1u) ? ~0u : 0u, (t1 & 2u) ? ~0u : 0u, (t1 & 4u) ? ~0u : 0u);
+          const word_t g = ju ^ si;
+          const word_t f0 = (g & hi) | (~g & lo);
+          A[i] = si ^ f0;
+          B[i] = lo ^ hi;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < Z; ++i) {
+        const int z = z0 + i;
+        if (z < L) {
+          prev = A[i] ^ (prev & B[i]);
+          own_w[z * zs] = prev;
+          if (z == 0) first = prev;
+        }
       }
     }
   }
@@ -269,7 +403,7 @@ __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, in
       const long jr = (long)(y + L * z) * hL + k;
       const word_t w = (open && xx == 0) ? 0 : (__ldg(x.J + (long)(0 + c) * x.half + jr) ^ si ^
                                                  x.sm[lrow(x, oc, z, yl) + kw * ns + slot]);
-      const word_t* pn = (yl > 0) ? x.sm + lrow(x, oc, z, yl - 1) : x.smN + lrow(x, oc, z, x.ny - 1);
+      const word_t* pn = (yl > 0) ? x.sm + lrow(x, oc, z, yl - 1) : x.smN + lrow_n(x, oc, z);
       const word_t n = __ldg(x.J + (long)(2 + c) * x.half + jr) ^ si ^ pn[k * ns + slot];
       word_t q0, q1;
       if (d3) {

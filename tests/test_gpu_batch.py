@@ -168,6 +168,40 @@ def test_large_single_slot_anneal_uses_big_clusters(sab, kernel):
         assert np.array_equal(b.spins(i, 0), o.spins())
 
 
+def test_uneven_cluster_row_split(sab):
+    """Instances whose y-rows do not divide evenly over their cluster's CTAs
+    (2D L=44 x 32 slots on 3 CTAs, 3D L=26 x 4 slots on 3 CTAs, a 3D L=46
+    single-slot anneal on 4 CTAs) reproduce the oracle."""
+    from simulated_annealing_b200.batch import Batch
+    b = Batch()
+    T32 = list(np.geomspace(0.3, 1.6, 32))
+    T4 = list(np.geomspace(0.5, 2.0, 4))
+    l32 = b.add_ladder(T32)
+    l4 = b.add_ladder(T4)
+    Ts = [2.5, 1.2]
+    sch = b.add_schedule(Ts, 2)
+    b.add_instance(O.LAT_2D, 44, ladder=l32, seed_J=61, seed=62)
+    b.add_instance(O.LAT_3D, 26, ladder=l4, seed_J=63, seed=64)
+    b.add_instance(O.LAT_3D, 46, schedule=sch, seed_J=65, seed=66)
+    b.finalize()
+    b.record_exchanges(16)
+    b.run(3)
+    b.run(2)
+    b.sync()
+    check_instance(b, 0, O.LAT_2D, 44, T32, 61, 62, 5)
+    check_instance(b, 1, O.LAT_3D, 26, T4, 63, 64, 5)
+    o = O.OracleSystem(O.LAT_3D, 46, mode=O.MODE_PHILOX)
+    o.set_seed(65)
+    o.init_J()
+    o.set_seed(66)
+    o.init_rand()
+    mn, _ = o.anneal(2.5, 1, 1.2, 2, 2, 1)
+    E, done = b.anneal_result(2)
+    assert done == 4
+    assert np.array_equal(E.astype(np.float32), mn)
+    assert np.array_equal(b.spins(2, 0), o.spins())
+
+
 def test_resident_groups(sab):
     """The C4 mix needs one launch per (lanes-per-site, cluster size) group."""
     from simulated_annealing_b200.batch import Batch
