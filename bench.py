@@ -22,6 +22,24 @@ roofline   algorithmic bytes per launch (per site and slot and sweep: spins read
 cpu_baseline / --impl reference: the reference's own CPU classes (cpu_2d,
            cpu_3d, parallel_tempering<>) compiled from its sources, on a bounded
            sample of the same instances, timed on this host.
+plain      the plain one-instance-per-launch form on the same GPU
+           (simulated_annealing_b200/sa_plain_pt: one system per slot, one launch
+           per half-sweep, a measurement copy per slot per sweep and a host
+           exchange per sweep, as parallel_tempering<gpu_sys> drives gpu_3d) on
+           a bounded sample of the same instances; batched_over_plain = value /
+           its rate.
+serving    continuous batching of anneal requests (simulated_annealing_b200.serve):
+           Poisson arrivals at 2,000/s, 2D L 16..128 or 3D L 8..64 with equal
+           probability (L log-uniform, rounded to even), sweeps log-uniform in
+           [1e3, 1e5], linear T 3.0 -> 0.2 in steps of 100 sweeps, couplings and
+           spins from per-request seeds; p50/p99 time from arrival to result on
+           the host clock and aggregate attempts/ns. The default run serves the
+           first --serve-requests requests of that stream; --workload serve runs
+           the whole 20,000.
+
+--workload c1|c2|c3 time the single-lattice cases instead (2D L=64 T=1.0 for
+10,000 sweeps; 3D L=32 anneal 3.0 -> 0.2 over 200 x 100 sweeps; 3D L=16
+32-temperature parallel tempering with an exchange every sweep).
 """
 from __future__ import annotations
 
@@ -202,6 +220,68 @@ def cpu_reference_sample(insts, budget_s: float, sweeps_per_instance: int = 50):
             "sample": sample}
 
 
+# ----------------------------------------------------------------------------- plain form
+def plain_sample(insts, budget_s: float, sweeps: int = 20):
+    """The plain one-instance-per-launch PT form over the first instances of the
+    workload (sa_plain_pt), until `budget_s` of timed loops."""
+    exe = os.path.join(ROOT, "simulated_annealing_b200", "sa_plain_pt")
+    lines = []
+    for lat, L, seed in insts:
+        T = LADDER_3D if lat == 2 else LADDER_2D
+        lines.append(f"{lat} {L} {seed} {len(T)} " + " ".join(repr(float(t)) for t in T))
+    r = subprocess.run([exe, str(budget_s), str(sweeps)], input="\n".join(lines) + "\n", capture_output=True,
+                       text=True, timeout=budget_s * 10 + 120)
+    if r.returncode != 0:
+        raise RuntimeError(f"sa_plain_pt failed: {r.stderr.strip()[-300:]}")
+    f = r.stdout.split()
+    done, att, sec = int(f[1]), float(f[3]), float(f[5])
+    return {"value": att / sec / 1e9, "unit": UNIT,
+            "sample": f"{done} instances of the mix x 16 slots x {sweeps} sweeps (+ exchange each sweep), "
+                      f"{sec:.1f} s of timed loops"}
+
+
+# ----------------------------------------------------------------------------- serving
+def c5_requests(n: int, rate: float, seed: int = 2000):
+    """The anneal-request stream: Poisson arrivals at `rate`/s (numpy PCG64 seed
+    `seed`), 2D L in [16,128] or 3D L in [8,64] with equal probability, L
+    log-uniform rounded to even, sweeps log-uniform in [1e3, 1e5] as steps of
+    100 sweeps on a linear T 3.0 -> 0.2 schedule, seeds 10000+k / 20000+k."""
+    from simulated_annealing_b200.serve import Request
+
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    out = []
+    for k in range(n):
+        two = rng.random() < 0.5
+        lo, hi = (16, 128) if two else (8, 64)
+        L = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi))) / 2)) * 2
+        L = max(lo, min(hi, L))
+        sweeps = float(np.exp(rng.uniform(np.log(1e3), np.log(1e5))))
+        steps = max(1, int(round(sweeps / 100)))
+        out.append(Request(float(t[k]), "2d" if two else "3d", L, 10_000 + k, 20_000 + k,
+                           np.linspace(3.0, 0.2, steps), 100))
+    return out
+
+
+def request_attempts(r) -> float:
+    N = r.L ** 3 if r.lattice == "3d" else r.L * r.L
+    return float(N) * 64 * len(r.T) * r.sweeps_per_step
+
+
+def serving_run(n: int, rate: float, budget_gb: float, chunk: int = 100):
+    from simulated_annealing_b200.serve import Server, run_open_loop
+
+    reqs = c5_requests(n, rate)
+    srv = Server(budget_bytes=int(budget_gb * (1 << 30)), max_requests=max(n, 1))
+    lat, res, wall = run_open_loop(srv, reqs, chunk=chunk)
+    srv.close()
+    att = sum(request_attempts(r) for r in reqs)
+    return {"requests": n, "arrival_rate_per_s": rate, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(np.mean(lat)), "wall_s": wall,
+            "attempts_per_ns": att / wall / 1e9, "budget_gb": budget_gb, "sweeps_per_round": chunk,
+            "latency": "arrival -> result on the host (host clock)"}
+
+
 # ----------------------------------------------------------------------------- GPU
 def run_ours(args):
     import torch
@@ -312,6 +392,12 @@ def run_ours(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_sample(insts, args.cpu_budget)
+        if world == 1 and args.plain_budget > 0:
+            pl = plain_sample(insts, args.plain_budget)
+            line["plain"] = pl
+            line["batched_over_plain"] = value / pl["value"]
+        if world == 1 and args.serve_requests > 0:
+            line["serving"] = serving_run(args.serve_requests, 2000.0, args.serve_budget_gb)
         print(json.dumps(line), flush=True)
     b.close()
     if dist:
@@ -346,6 +432,81 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_single(args):
+    """One JSON line for the serving stream or a single-lattice case."""
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    base = {"n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64 (bitwise/int32)", "data": "synthetic"}
+    if args.workload == "serve":
+        clocks.start()
+        r = serving_run(20_000, 2000.0, 120.0)
+        line = dict(base, metric="anneal time-to-result p99 (s)", value=r["p99_s"], unit="s",
+                    higher_is_better=False, config={"workload": "serving: 20,000 anneal requests, Poisson 2,000/s"},
+                    serving=r)
+        line["clocks"] = clocks.stop()
+        print(json.dumps(line), flush=True)
+        return
+    from simulated_annealing_b200.batch import Batch
+    from simulated_annealing_b200.system import GpuSystem
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream()
+    if args.workload == "c1":
+        s = GpuSystem("2d", 64, 1.0)
+        s.set_seed(1); s.init_J(); s.set_seed(2); s.init_rand()
+        for _ in range(args.warmup):
+            s.sweep(1000)
+        s.sync()
+        clocks.start()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            s.sweep(10_000)
+        s.sync()
+        dt = time.perf_counter() - t0
+        att = 10_000 * 4096 * 64 * args.steps
+        wl = "2D L=64 periodic, T=1.0, 10,000 sweeps per step (one launch per half-sweep)"
+    elif args.workload == "c2":
+        s = GpuSystem("3d", 32, 3.0)
+        s.set_seed(3); s.init_J(); s.set_seed(3); s.init_rand()
+        T = np.linspace(3.0, 0.2, 200)
+        for _ in range(args.warmup):
+            s.anneal(T[:10], 100, 1)
+        s.sync()
+        clocks.start()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            s.anneal(T, 100, 1)
+        s.sync()
+        dt = time.perf_counter() - t0
+        att = 20_000 * 32768 * 64 * args.steps
+        wl = "3D L=32 anneal, linear T 3.0 -> 0.2 over 200 steps x 100 sweeps, measure every sweep"
+    else:
+        b = Batch()
+        lad = b.add_ladder(np.geomspace(0.5, 2.0, 32))
+        b.add_instance(2, 16, ladder=lad, seed_J=4, seed=4)
+        b.finalize()
+        b.set_stream(stream.cuda_stream)
+        S = 10_000
+        for _ in range(args.warmup):
+            b.run(1000)
+        b.sync()
+        clocks.start()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            b.run(S)
+        b.sync()
+        dt = time.perf_counter() - t0
+        att = S * 4096 * 32 * 64 * args.steps
+        wl = "3D L=16 x 32 temperatures (geometric 0.5-2.0), exchange every sweep, 10,000 sweeps per step"
+    clk = clocks.stop()
+    line = dict(base, metric=METRIC, value=att / dt / 1e9, unit=UNIT, ms_per_step=dt * 1e3 / args.steps,
+                config={"workload": wl, "timing": "host clock around synchronised steps"}, clocks=clk)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,7 +518,13 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-step-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-budget", type=float, default=8.0, help="seconds of the plain form (0 = skip)")
+    ap.add_argument("--serve-requests", type=int, default=300, help="requests in the serving sample (0 = skip)")
+    ap.add_argument("--serve-budget-gb", type=float, default=16.0)
+    ap.add_argument("--workload", choices=["c4", "serve", "c1", "c2", "c3"], default="c4")
     args = ap.parse_args()
+    if args.workload != "c4" and args.impl == "ours":
+        return run_single(args)
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":

@@ -21,6 +21,8 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <set>
 #include <random>
 #include <string>
 #include <vector>
@@ -967,7 +969,10 @@ static int launch_group(sa_batch* b, const sa_batch::Group& g, int gi, long nswe
 template <int P>
 static int prepare_resident(const sa_batch::Group& g, size_t smem_limit, int* max_clusters) {
   void (*kern)(BatchParams) = resident_kernel<P>(g);
-  SA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit));
+  // the attribute is a ceiling shared by every user of the variant in the
+  // process (batches and servers): never lower it below the whole budget
+  SA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)std::max(smem_limit, kResSmemBudget)));
   SA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)g.C, 1, 1);
@@ -995,9 +1000,27 @@ static int prepare_resident(const sa_batch::Group& g, size_t smem_limit, int* ma
   return SA_OK;
 }
 
+// Serving: the kernel variant's attributes are set once, to the whole shared
+// memory budget, so rounds with new shapes need no further attribute calls.
+template <int P>
+static int prepare_resident_once(const sa_batch::Group& g) {
+  static std::mutex mu;
+  static std::set<std::pair<int, void*>> done;
+  void (*kern)(BatchParams) = resident_kernel<P>(g);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({dev, (void*)kern})) return SA_OK;
+  SA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kResSmemBudget));
+  SA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  done.insert({dev, (void*)kern});
+  return SA_OK;
+}
+
 template <int P>
 static int group_dispatch(sa_batch* b, const sa_batch::Group& g, int gi, long nsweeps, int prepare,
                           int* max_clusters) {
+  if (prepare == 2) return g.resident ? prepare_resident_once<P>(g) : SA_OK;
   if (prepare) {
     if (!g.resident) return SA_OK;
     size_t lim = 0;
@@ -1636,9 +1659,10 @@ int sa_serve_create(size_t budget_bytes, int max_requests, sa_serve_t* out) {
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&b.own_stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
   b.stream = b.own_stream;
-  // budget: 1/16 for thresholds (64 B each), states (~1.1 KB each), the rest words
+  // budget: 1/64 for thresholds (64 B per schedule step), the request states
+  // (~1.1 KB each), the rest spin and coupling words
   const size_t state_bytes = (size_t)max_requests * sizeof(InstState);
-  const size_t thr_bytes = budget_bytes / 16;
+  const size_t thr_bytes = budget_bytes / 64;
   if (state_bytes + thr_bytes >= budget_bytes) {
     delete s;
     return fail(SA_ERR_BUDGET, "budget too small for the request table");
@@ -1827,7 +1851,7 @@ int sa_serve_run(sa_serve_t s, long nsweeps) {
     g.done = s->events[gi];
     if (g.resident) {
       int mc = 0;
-      int st = dispatch(&b, g, (int)gi, 0, 1, &mc);  // kernel attributes (cheap after the first time)
+      int st = dispatch(&b, g, (int)gi, 0, 2, &mc);  // kernel attributes, once per variant
       if (st) return st;
     } else {
       g.grid = (int)std::min<int64_t>((int64_t)sms, (int64_t)g.count);
