@@ -406,9 +406,12 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
   if (CL) {
     x.smN = cluster.map_shared_rank(s_spins, (unsigned)((q + C - 1) % C));
     x.smS = cluster.map_shared_rank(s_spins, (unsigned)((q + 1) % C));
+    x.smNA = cluster_addr(smem_addr(s_spins), (unsigned)((q + C - 1) % C));
+    x.smSA = cluster_addr(smem_addr(s_spins), (unsigned)((q + 1) % C));
   } else {
     x.smN = s_spins;
     x.smS = s_spins;
+    x.smNA = x.smSA = smem_addr(s_spins);
   }
   x.J = p.J + d.J_off;
   constexpr bool d3 = LAT == SA_LATTICE_3D, open = LAT == SA_LATTICE_2D_OPEN_X;
@@ -453,10 +456,10 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
     }
     for (int c = 0; c < 2; ++c) {
       if (d3) {
-        if (P == 1 && SL == 1 && x.L > 4) rhalf_3d1<4>(x, c, draw + c, th[0]);
-        else rhalf_3d<P, SL>(x, c, draw + c, th);
+        if (P == 1 && SL == 1 && x.L > 4) rhalf_3d1<4, CL>(x, c, draw + c, th[0]);
+        else rhalf_3d<P, SL, CL>(x, c, draw + c, th);
       }
-      else rhalf_2d<P, SL, open>(x, c, draw + c, th, tb);
+      else rhalf_2d<P, SL, open, CL>(x, c, draw + c, th, tb);
       sync_all();
     }
     draw += 2;
@@ -467,7 +470,7 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
     if (p.hist && d.hist_off >= 0 && sweeps % p.hstride == 0) {
       for (int a = 0; a < d.nslots; a += 2) {
         const int nh = (a + 1 < d.nslots) ? 2 : 1;
-        rmeasure(x, d3, open, a, nh, s_cnt);
+        rmeasure<CL>(x, d3, open, a, nh, s_cnt);
         sync_all();
         if (q == 0 && threadIdx.x < 64 * nh) {
           const int qq = threadIdx.x >> 6, j = threadIdx.x & 63;
@@ -493,7 +496,7 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
         a = dc.pair;
         nsl = 2;
       }
-      rmeasure(x, d3, open, a, nsl, s_cnt);
+      rmeasure<CL>(x, d3, open, a, nsl, s_cnt);
       sync_all();
       if (threadIdx.x < 128) {
         unsigned v = 0;

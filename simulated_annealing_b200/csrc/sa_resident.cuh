@@ -35,6 +35,7 @@ struct ResCtx {
   uint64_t seed;
   int L, hL, ny, y0, ns, zc;  // zc: z-planes (L in 3D, 1 in 2D)
   int nyN, nyS;               // rows held by the CTAs owning y0-1 and y0+ny
+  uint32_t smNA, smSA;        // shared::cluster byte addresses of those CTAs' spins
   int half;                   // sites per colour of the instance (global J stride)
   int rowW;                   // words per local row: hL*ns
   uint32_t magic;             // floor(2^32/hL)+1, for division by hL
@@ -86,10 +87,82 @@ __device__ __forceinline__ void stw(word_t* p, const SlotWords<SL>& v) {
   else p[0] = v.w[0];
 }
 
+// Cluster shared-memory access. A neighbour row is read through its 32-bit
+// shared::cluster address with ld.shared::cluster (a local row's shared::cta
+// address is a valid cluster address of the executing CTA), so the loads keep
+// 32-bit address arithmetic and never go through generic addressing.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t a, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+
+template <int SL>
+__device__ __forceinline__ SlotWords<SL> ldc(uint32_t a) {
+  SlotWords<SL> r;
+  if (SL == 2) {
+    unsigned long long v0, v1;
+    asm volatile("ld.shared::cluster.v2.u64 {%0, %1}, [%2];" : "=l"(v0), "=l"(v1) : "r"(a));
+    r.w[0] = v0;
+    r.w[SL - 1] = v1;
+  } else {
+    unsigned long long v0;
+    asm volatile("ld.shared::cluster.u64 %0, [%1];" : "=l"(v0) : "r"(a));
+    r.w[0] = v0;
+  }
+  return r;
+}
+
+// A row of the other colour north or south of a site row: local, or (CL)
+// possibly in the neighbouring CTA. off / step are in words.
+template <bool CL>
+struct NbRow;
+
+template <>
+struct NbRow<false> {
+  const word_t* p;
+  template <int SL>
+  __device__ __forceinline__ SlotWords<SL> ld(int off) const { return ldw<SL>(p + off); }
+  __device__ __forceinline__ void step(int words) { p += words; }
+};
+
+template <>
+struct NbRow<true> {
+  uint32_t a;
+  template <int SL>
+  __device__ __forceinline__ SlotWords<SL> ld(int off) const { return ldc<SL>(a + 8u * (uint32_t)off); }
+  __device__ __forceinline__ void step(int words) { a += 8u * (uint32_t)words; }
+};
+
+// row y_local-1 (north) / y_local+1 (south) of colour oc in plane z
+template <bool CL>
+__device__ __forceinline__ NbRow<CL> north_row(const ResCtx& x, int oc, int z, int yl) {
+  NbRow<CL> r;
+  if constexpr (CL) {
+    r.a = (yl > 0) ? smem_addr(x.sm + lrow(x, oc, z, yl - 1)) : x.smNA + 8u * (uint32_t)lrow_n(x, oc, z);
+  } else {
+    r.p = (yl > 0) ? x.sm + lrow(x, oc, z, yl - 1) : x.smN + lrow_n(x, oc, z);
+  }
+  return r;
+}
+
+template <bool CL>
+__device__ __forceinline__ NbRow<CL> south_row(const ResCtx& x, int oc, int z, int yl) {
+  NbRow<CL> r;
+  if constexpr (CL) {
+    r.a = (yl < x.ny - 1) ? smem_addr(x.sm + lrow(x, oc, z, yl + 1)) : x.smSA + 8u * (uint32_t)lrow_s(x, oc, z);
+  } else {
+    r.p = (yl < x.ny - 1) ? x.sm + lrow(x, oc, z, yl + 1) : x.smS + lrow_s(x, oc, z);
+  }
+  return r;
+}
+
 // Lanes: (site group lane/P, slots (lane%P)*SL .. +SL-1). All slots of a site
 // share the coupling loads and the site's Philox draw; SL > 1 requires an
 // even slot count (16-byte aligned slot pairs).
-template <int P, int SL, bool OPEN_X>
+template <int P, int SL, bool OPEN_X, bool CL>
 __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, const uint32_t (*th)[8],
                                          const uint32_t (*tb)[8]) {
   constexpr int SPS = 32 / P;
@@ -125,14 +198,13 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
         x_neighbours(k, par, hL, kw, ke);
         const int own = lrow(x, c, 0, yl) + k * ns + slot;
         const int orow = lrow(x, oc, 0, yl);
-        const word_t* pn = (yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow_n(x, oc, 0);
-        const word_t* ps = (yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow_s(x, oc, 0);
+        const NbRow<CL> pn = north_row<CL>(x, oc, 0, yl), ps = south_row<CL>(x, oc, 0, yl);
         const int ys = (y == L - 1) ? 0 : y + 1;
         const SlotWords<SL> si = ldw<SL>(x.sm + own);
         const SlotWords<SL> sw = ldw<SL>(x.sm + orow + kw * ns + slot);
         const SlotWords<SL> se = ldw<SL>(x.sm + orow + ke * ns + slot);
-        const SlotWords<SL> sn = ldw<SL>(pn + k * ns + slot);
-        const SlotWords<SL> ss = ldw<SL>(ps + k * ns + slot);
+        const SlotWords<SL> sn = pn.template ld<SL>(k * ns + slot);
+        const SlotWords<SL> ss = ps.template ld<SL>(k * ns + slot);
         const word_t jw = __ldg(Jxc + y * hL + k), je = __ldg(Jxo + y * hL + ke);
         const word_t jn = __ldg(Jyc + y * hL + k), js = __ldg(Jyo + ys * hL + k);
         const bool border = OPEN_X && (xx == 0 || xx == L - 1);
@@ -159,7 +231,7 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
   }
 }
 
-template <int P, int SL>
+template <int P, int SL, bool CL>
 __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, const uint32_t (*th)[8]) {
   constexpr int SPS = 32 / P;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -190,8 +262,9 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
     int own = lrow(x, c, 0, yl) + k * ns + slot;
     int ow = lrow(x, oc, 0, yl) + kw * ns + slot;
     int oe = lrow(x, oc, 0, yl) + ke * ns + slot;
-    const word_t* pn = ((yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow_n(x, oc, 0)) + k * ns + slot;
-    const word_t* ps = ((yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow_s(x, oc, 0)) + k * ns + slot;
+    NbRow<CL> pn = north_row<CL>(x, oc, 0, yl), ps = south_row<CL>(x, oc, 0, yl);
+    pn.step(k * ns + slot);
+    ps.step(k * ns + slot);
     const int zsn = (yl > 0) ? zs : x.nyN * x.rowW;       // z stride of the north row's owner
     const int zss = (yl < x.ny - 1) ? zs : x.nyS * x.rowW;
     int jo = y * hL + k, je = y * hL + ke, js = ys * hL + k;
@@ -214,8 +287,8 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
           const SlotWords<SL> sd = last ? first : ldw<SL>(x.sm + own + zs);
           const SlotWords<SL> sw = ldw<SL>(x.sm + ow);
           const SlotWords<SL> se = ldw<SL>(x.sm + oe);
-          const SlotWords<SL> sn = ldw<SL>(pn);
-          const SlotWords<SL> ss = ldw<SL>(ps);
+          const SlotWords<SL> sn = pn.template ld<SL>(0);
+          const SlotWords<SL> ss = ps.template ld<SL>(0);
           const word_t jw = __ldg(Jxc + jo), je_ = __ldg(Jxo + je), jn = __ldg(Jyc + jo);
           const word_t js_ = __ldg(Jyo + js), ju = __ldg(Jzc + jo);
           const word_t jd = __ldg(Jzc + (last ? jo - (L - 1) * zg : jo + zg));
@@ -236,8 +309,8 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         own += zs;
         ow += zs;
         oe += zs;
-        pn += zsn;
-        ps += zss;
+        pn.step(zsn);
+        ps.step(zss);
         jo += zg;
         je += zg;
         js += zg;
@@ -287,7 +360,7 @@ __device__ __forceinline__ word_t below(word_t c0, word_t c1, word_t c2, uint32_
 // applies Z maps at two logic operations each. The top plane's z+1
 // neighbour is the new z = 0 spin, known once the first chunk is applied
 // (requires L > Z).
-template <int Z>
+template <int Z, bool CL>
 __device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw, const uint32_t* th) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int L = x.L, hL = x.hL;
@@ -313,8 +386,9 @@ __device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw,
     const word_t* own = x.sm + lrow(x, c, 0, yl) + k;
     const word_t* pw = x.sm + lrow(x, oc, 0, yl) + kw;
     const word_t* pe = x.sm + lrow(x, oc, 0, yl) + ke;
-    const word_t* pn = ((yl > 0) ? x.sm + lrow(x, oc, 0, yl - 1) : x.smN + lrow_n(x, oc, 0)) + k;
-    const word_t* ps = ((yl < x.ny - 1) ? x.sm + lrow(x, oc, 0, yl + 1) : x.smS + lrow_s(x, oc, 0)) + k;
+    NbRow<CL> pn = north_row<CL>(x, oc, 0, yl), ps = south_row<CL>(x, oc, 0, yl);
+    pn.step(k);
+    ps.step(k);
     const int zsn = (yl > 0) ? zs : x.nyN * x.rowW;
     const int zss = (yl < x.ny - 1) ? zs : x.nyS * x.rowW;
     const int jo = y * hL + k, je = y * hL + ke, js = ys * hL + k;
@@ -335,7 +409,7 @@ __device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw,
           const word_t si = own[z * zs];
           const word_t sd = last ? first : own[zn * zs];
           const word_t sw = pw[z * zs], se = pe[z * zs];
-          const word_t sn = pn[z * zsn], ss = ps[z * zss];
+          const word_t sn = pn.template ld<1>(z * zsn).w[0], ss = ps.template ld<1>(z * zss).w[0];
           const word_t jw = __ldg(Jxc + jo + z * zg), jee = __ldg(Jxo + je + z * zg);
           const word_t jn = __ldg(Jyc + jo + z * zg), jss = __ldg(Jyo + js + z * zg);
           const word_t ju = __ldg(Jzc + jo + z * zg), jd = __ldg(Jzc + jo + zn * zg);
@@ -370,6 +444,7 @@ __device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw,
 
 // Partial satisfied-bond counts of slots a..a+nsl-1 over this CTA's sites
 // (each bond counted once, from its site towards -x/-y/-z) into cnt[q][j].
+template <bool CL>
 __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, int a, int nsl,
                                          unsigned (*cnt)[64]) {
   for (int i = threadIdx.x; i < 128; i += blockDim.x) (&cnt[0][0])[i] = 0;
@@ -403,8 +478,8 @@ __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, in
       const long jr = (long)(y + L * z) * hL + k;
       const word_t w = (open && xx == 0) ? 0 : (__ldg(x.J + (long)(0 + c) * x.half + jr) ^ si ^
                                                  x.sm[lrow(x, oc, z, yl) + kw * ns + slot]);
-      const word_t* pn = (yl > 0) ? x.sm + lrow(x, oc, z, yl - 1) : x.smN + lrow_n(x, oc, z);
-      const word_t n = __ldg(x.J + (long)(2 + c) * x.half + jr) ^ si ^ pn[k * ns + slot];
+      const NbRow<CL> pn = north_row<CL>(x, oc, z, yl);
+      const word_t n = __ldg(x.J + (long)(2 + c) * x.half + jr) ^ si ^ pn.template ld<1>(k * ns + slot).w[0];
       word_t q0, q1;
       if (d3) {
         const int zu = (z == 0) ? L - 1 : z - 1;
