@@ -414,16 +414,26 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
     x.smNA = x.smSA = smem_addr(s_spins);
   }
   x.J = p.J + d.J_off;
+  const bool pow2 = (d.nslots & (d.nslots - 1)) == 0;
+  x.swsh = SL - 1;
+  x.swm = (pow2 && d.nslots > 1) ? ((d.nslots - 1) & ~(SL - 1)) : 0;
+  const int lg_ns = __ffs(d.nslots) - 1;  // used only when swizzled (power-of-two slot count)
+  // word i of a (colour, plane) block in the global order -> its swizzled place
+  auto phys = [&](int i) -> int {
+    if (!x.swm) return i;
+    const int site = i >> lg_ns;
+    return i ^ swz(x, site - div_hl(site, x) * x.hL);
+  };
   constexpr bool d3 = LAT == SA_LATTICE_3D, open = LAT == SA_LATTICE_2D_OPEN_X;
 
-  // global [colour][row = y + L*z][k][slot] -> local [colour][z][y_local][k][slot]
+  // global [colour][row = y + L*z][k][slot] -> local [colour][z][y_local][k][slot ^ swizzle]
   word_t* gS = p.spins + d.spin_off;
   const int blk = x.ny * x.rowW;
   for (int cz = 0; cz < 2 * x.zc; ++cz) {
     const int c = cz / x.zc, z = cz - c * x.zc;
     const word_t* src = gS + ((long)c * d.half + (long)(z * x.L + x.y0) * x.hL) * x.ns;
     word_t* dst = s_spins + (long)cz * blk;
-    for (int i = threadIdx.x; i < blk; i += blockDim.x) dst[i] = src[i];
+    for (int i = threadIdx.x; i < blk; i += blockDim.x) dst[phys(i)] = src[i];
   }
   sync_all();
 
@@ -521,11 +531,12 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
         if (mask) {
           const int nloc = 2 * x.zc * x.ny * x.hL;
           for (int t = threadIdx.x; t < nloc; t += blockDim.x) {
-            word_t* w = s_spins + (long)t * x.ns + a;
-            const word_t x0 = w[0], x1 = w[1];
+            word_t* w = s_spins + (long)t * x.ns;
+            const int sw = x.swm ? swz(x, t - div_hl(t, x) * x.hL) : 0;  // t % hL is the site's k
+            const word_t x0 = w[a ^ sw], x1 = w[(a + 1) ^ sw];
             const word_t dd = (x0 ^ x1) & mask;
-            w[0] = x0 ^ dd;
-            w[1] = x1 ^ dd;
+            w[a ^ sw] = x0 ^ dd;
+            w[(a + 1) ^ sw] = x1 ^ dd;
           }
         }
         if (q == 0 && threadIdx.x == 0) {
@@ -553,7 +564,7 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
     const int c = cz / x.zc, z = cz - c * x.zc;
     word_t* dst = gS + ((long)c * d.half + (long)(z * x.L + x.y0) * x.hL) * x.ns;
     const word_t* src = s_spins + (long)cz * blk;
-    for (int i = threadIdx.x; i < blk; i += blockDim.x) dst[i] = src[i];
+    for (int i = threadIdx.x; i < blk; i += blockDim.x) dst[i] = src[phys(i)];
   }
   if (q == 0 && threadIdx.x == 0) {
     st->draw = draw;

@@ -36,6 +36,7 @@ struct ResCtx {
   int L, hL, ny, y0, ns, zc;  // zc: z-planes (L in 3D, 1 in 2D)
   int nyN, nyS;               // rows held by the CTAs owning y0-1 and y0+ny
   uint32_t smNA, smSA;        // shared::cluster byte addresses of those CTAs' spins
+  int swm, swsh;              // slot swizzle: slot s of site k sits at s ^ ((k << swsh) & swm)
   int half;                   // sites per colour of the instance (global J stride)
   int rowW;                   // words per local row: hL*ns
   uint32_t magic;             // floor(2^32/hL)+1, for division by hL
@@ -53,6 +54,14 @@ __device__ __forceinline__ int div_hl(int t, const ResCtx& x) {
 __device__ __forceinline__ int lrow(const ResCtx& x, int c, int z, int yl) {
   return ((c * x.zc + z) * x.ny + yl) * x.rowW;
 }
+
+// Slot swizzle. Slots are innermost (a site's ns words are contiguous), so a
+// warp reading ONE slot of many sites (the exchange energies, the swap) would
+// hit the same two banks ns/2-fold. With a power-of-two slot count the slot
+// index is XORed with the site's k (in pairs when lanes access two slots at
+// once), which keeps a site's words in its own ns-word block while spreading
+// one slot over all banks.
+__device__ __forceinline__ int swz(const ResCtx& x, int k) { return (k << x.swsh) & x.swm; }
 
 // the halo rows: last row of the north neighbour, first row of the south one
 __device__ __forceinline__ int lrow_n(const ResCtx& x, int c, int z) {
@@ -196,15 +205,16 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
         const int par = (c + y) & 1, xx = 2 * k + par;
         int kw, ke;
         x_neighbours(k, par, hL, kw, ke);
-        const int own = lrow(x, c, 0, yl) + k * ns + slot;
+        const int sk = slot ^ swz(x, k);
+        const int own = lrow(x, c, 0, yl) + k * ns + sk;
         const int orow = lrow(x, oc, 0, yl);
         const NbRow<CL> pn = north_row<CL>(x, oc, 0, yl), ps = south_row<CL>(x, oc, 0, yl);
         const int ys = (y == L - 1) ? 0 : y + 1;
         const SlotWords<SL> si = ldw<SL>(x.sm + own);
-        const SlotWords<SL> sw = ldw<SL>(x.sm + orow + kw * ns + slot);
-        const SlotWords<SL> se = ldw<SL>(x.sm + orow + ke * ns + slot);
-        const SlotWords<SL> sn = pn.template ld<SL>(k * ns + slot);
-        const SlotWords<SL> ss = ps.template ld<SL>(k * ns + slot);
+        const SlotWords<SL> sw = ldw<SL>(x.sm + orow + kw * ns + (slot ^ swz(x, kw)));
+        const SlotWords<SL> se = ldw<SL>(x.sm + orow + ke * ns + (slot ^ swz(x, ke)));
+        const SlotWords<SL> sn = pn.template ld<SL>(k * ns + sk);
+        const SlotWords<SL> ss = ps.template ld<SL>(k * ns + sk);
         const word_t jw = __ldg(Jxc + y * hL + k), je = __ldg(Jxo + y * hL + ke);
         const word_t jn = __ldg(Jyc + y * hL + k), js = __ldg(Jyo + ys * hL + k);
         const bool border = OPEN_X && (xx == 0 || xx == L - 1);
@@ -259,12 +269,13 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
     x_neighbours(k, par, hL, kw, ke);
     const int ys = (y == L - 1) ? 0 : y + 1;
     // z = 0 offsets; every z step adds zs (shared) or zg (couplings)
-    int own = lrow(x, c, 0, yl) + k * ns + slot;
-    int ow = lrow(x, oc, 0, yl) + kw * ns + slot;
-    int oe = lrow(x, oc, 0, yl) + ke * ns + slot;
+    const int sk = slot ^ swz(x, k);
+    int own = lrow(x, c, 0, yl) + k * ns + sk;
+    int ow = lrow(x, oc, 0, yl) + kw * ns + (slot ^ swz(x, kw));
+    int oe = lrow(x, oc, 0, yl) + ke * ns + (slot ^ swz(x, ke));
     NbRow<CL> pn = north_row<CL>(x, oc, 0, yl), ps = south_row<CL>(x, oc, 0, yl);
-    pn.step(k * ns + slot);
-    ps.step(k * ns + slot);
+    pn.step(k * ns + sk);
+    ps.step(k * ns + sk);
     const int zsn = (yl > 0) ? zs : x.nyN * x.rowW;       // z stride of the north row's owner
     const int zss = (yl < x.ny - 1) ? zs : x.nyS * x.rowW;
     int jo = y * hL + k, je = y * hL + ke, js = ys * hL + k;
@@ -474,16 +485,17 @@ __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, in
       int kw, ke;
       x_neighbours(k, par, hL, kw, ke);
       const int oc = 1 - c;
-      const word_t si = x.sm[lrow(x, c, z, yl) + k * ns + slot];
+      const int sk = slot ^ swz(x, k);
+      const word_t si = x.sm[lrow(x, c, z, yl) + k * ns + sk];
       const long jr = (long)(y + L * z) * hL + k;
       const word_t w = (open && xx == 0) ? 0 : (__ldg(x.J + (long)(0 + c) * x.half + jr) ^ si ^
-                                                 x.sm[lrow(x, oc, z, yl) + kw * ns + slot]);
+                                                 x.sm[lrow(x, oc, z, yl) + kw * ns + (slot ^ swz(x, kw))]);
       const NbRow<CL> pn = north_row<CL>(x, oc, z, yl);
-      const word_t n = __ldg(x.J + (long)(2 + c) * x.half + jr) ^ si ^ pn.template ld<1>(k * ns + slot).w[0];
+      const word_t n = __ldg(x.J + (long)(2 + c) * x.half + jr) ^ si ^ pn.template ld<1>(k * ns + sk).w[0];
       word_t q0, q1;
       if (d3) {
         const int zu = (z == 0) ? L - 1 : z - 1;
-        const word_t uu = __ldg(x.J + (long)(4 + c) * x.half + jr) ^ si ^ x.sm[lrow(x, c, zu, yl) + k * ns + slot];
+        const word_t uu = __ldg(x.J + (long)(4 + c) * x.half + jr) ^ si ^ x.sm[lrow(x, c, zu, yl) + k * ns + sk];
         q0 = w ^ n ^ uu;
         q1 = (w & n) | (uu & (w ^ n));
       } else {
