@@ -451,7 +451,22 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
   }
   uint64_t draw = draw0;
   int64_t sweeps = sweeps0, xsteps = xsteps0;
+  // per-launch accumulators, written back once at the end: exchange counters
+  // per pair (smem) and the anneal record (registers of threads 0..63 of rank 0)
+  __shared__ int64_t s_acc[32], s_att[32];
+  for (int t = threadIdx.x; t < 32; t += blockDim.x) s_acc[t] = s_att[t] = 0;
+  int64_t my_emax = 0, my_elast = 0, measured = 0;
+  if (d.sched >= 0 && q == 0 && threadIdx.x < 64) {
+    my_emax = st->emax[threadIdx.x];
+    my_elast = st->elast[threadIdx.x];
+  }
+  if (d.sched >= 0) measured = st->measured;
+  __syncthreads();
   for (int64_t i = 0; i < n; ++i) {
+    // this sweep's exchange decision, fetched before the half-sweeps hide its latency
+    const bool xchg = d.ladder >= 0 && d.nslots > 1 && (sweeps + 1) % p.xinterval == 0;
+    Decision dc = {0, 0, 0, 0};
+    if (xchg) dc = p.dec[d.dec_off + xsteps];
     if (d.sched >= 0) {
       int64_t s = sweeps / d.sweeps_per_step;
       if (s > d.thr_count - 1) s = d.thr_count - 1;
@@ -496,13 +511,10 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
         sync_all();
       }
     }
-    const bool xchg = d.ladder >= 0 && d.nslots > 1 && sweeps % p.xinterval == 0;
     const bool meas = d.sched >= 0 && p.mstride > 0 && in_step % p.mstride == 0;
     if (xchg || meas) {
-      Decision dc = {0, 0, 0, 0};
       int a = 0, nsl = 1;
       if (xchg) {
-        dc = p.dec[d.dec_off + xsteps];
         a = dc.pair;
         nsl = 2;
       }
@@ -540,8 +552,8 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
           }
         }
         if (q == 0 && threadIdx.x == 0) {
-          p.acc[d.pair_off + a] += __popcll(mask);
-          p.att[d.pair_off + a] += 1;
+          s_acc[a] += __popcll(mask);
+          s_att[a] += 1;
           if (p.rec_pair && xsteps < p.rec_cap) {
             p.rec_pair[(long)id * p.rec_cap + xsteps] = a;
             p.rec_mask[(long)id * p.rec_cap + xsteps] = mask;
@@ -549,14 +561,12 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
         }
         xsteps += 1;
       } else if (q == 0 && threadIdx.x < 64) {
-        const int j = threadIdx.x;
-        const int64_t e = 2 * (int64_t)s_tot[0][j] - d.nbonds;
-        const int64_t m0 = st->measured;
-        st->elast[j] = e;
-        st->emax[j] = (m0 == 0) ? e : max(st->emax[j], e);
+        const int64_t e = 2 * (int64_t)s_tot[0][threadIdx.x] - d.nbonds;
+        my_elast = e;
+        my_emax = (measured == 0) ? e : max(my_emax, e);
       }
       sync_all();
-      if (meas && q == 0 && threadIdx.x == 0) st->measured += 1;
+      if (meas) measured += 1;
     }
   }
   // local -> global
@@ -566,10 +576,22 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
     const word_t* src = s_spins + (long)cz * blk;
     for (int i = threadIdx.x; i < blk; i += blockDim.x) dst[i] = src[phys(i)];
   }
-  if (q == 0 && threadIdx.x == 0) {
-    st->draw = draw;
-    st->sweeps = sweeps;
-    st->xsteps = xsteps;
+  if (q == 0) {
+    if (threadIdx.x == 0) {
+      st->draw = draw;
+      st->sweeps = sweeps;
+      st->xsteps = xsteps;
+      if (d.sched >= 0) st->measured = measured;
+    }
+    if (d.sched >= 0 && threadIdx.x < 64) {
+      st->emax[threadIdx.x] = my_emax;
+      st->elast[threadIdx.x] = my_elast;
+    }
+    if (d.ladder >= 0)
+      for (int t = threadIdx.x; t < d.nslots - 1; t += blockDim.x) {
+        p.acc[d.pair_off + t] += s_acc[t];
+        p.att[d.pair_off + t] += s_att[t];
+      }
   }
   sync_all();  // no CTA leaves while a peer may still read its shared memory
 }
