@@ -71,6 +71,24 @@ def c4_instances(n: int, index_offset: int = 0):
     return [(SHAPES[p][0], SHAPES[p][1], 1000 + index_offset + k) for k, p in enumerate(picks)]
 
 
+def shard_instances(rank: int, world: int, n: int):
+    """Rank `rank`'s share of a `world`-rank run: instances [rank*n, (rank+1)*n)
+    of the global sequence (weak scaling: n per rank, no overlap)."""
+    assert 0 <= rank < world
+    return c4_instances(n, index_offset=rank * n)
+
+
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of per-rank timings (the whole job ends when the
+    slowest rank does)."""
+    import torch
+
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
 def site_count(lat: int, L: int) -> int:
     return L ** 3 if lat == 2 else L * L
 
@@ -301,7 +319,7 @@ def run_ours(args):
 
     from simulated_annealing_b200.batch import Batch
 
-    insts = c4_instances(args.instances, index_offset=rank * args.instances)
+    insts = shard_instances(rank, world, args.instances)
     b = Batch()
     l2 = b.add_ladder(LADDER_2D)
     l3 = b.add_ladder(LADDER_3D)
@@ -354,10 +372,7 @@ def run_ours(args):
     t_e2e = time.perf_counter() - t0
     barrier()
 
-    times = torch.tensor([ms, t_e2e * 1e3], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = float(times[0]), float(times[1])
+    ms, e2e_ms = max_over_ranks([ms, t_e2e * 1e3], dist, "cuda")
     total_attempts = attempts_step * args.steps * world
     value = total_attempts / (ms * 1e6)
     e2e_value = total_attempts / (e2e_ms * 1e6)

@@ -9,7 +9,7 @@
 // the reference CPU path as its CPU baseline.
 //
 // State is read back through the reference's own save() stream
-// (src/cpu_2dp.cpp:508-519, src/cpu_3d.cpp:516-528). Parallel-tempering
+// (src/cpu_2dp.cpp:444-456, src/cpu_3d.cpp:449-461). Parallel-tempering
 // decisions are observed by wrapping each system in a forwarding cpu_sys that
 // records the (pair, mask) the reference template passes to swap()
 // (src/parallel_tempering.hpp:112-114).

@@ -8,15 +8,15 @@
 // What it restates (reference paths are relative to the reference project):
 //   * lattice bit logic      src/cpu_2d.cpp:5-41 (2D periodic),
 //                            src/cpu_2dp.cpp:336-383 (2D open in x),
-//                            src/cpu_3d.cpp:174-228 (3D periodic)
-//   * sweep order            src/cpu_2dp.cpp:106-114, src/cpu_3d.cpp:161-172
+//                            src/cpu_3d.cpp:107-161 (3D periodic)
+//   * sweep order            src/cpu_2dp.cpp:106-114, src/cpu_3d.cpp:94-105
 //                            (colour (x+y)%2 in BOTH 2D and 3D; in 3D the z
 //                            neighbours share a colour, so each half-sweep is
 //                            sequential along z inside every (x,y) column)
-//   * Boltzmann tables       src/cpu_2dp.cpp:33-40, src/cpu_3d.cpp:99-104
+//   * Boltzmann tables       src/cpu_2dp.cpp:33-40, src/cpu_3d.cpp:218-232
 //   * measure (-H)           src/cpu_2d.cpp:67-94, src/cpu_2dp.cpp:196-214,
-//                            src/cpu_3d.cpp:400-438
-//   * J layout / generation  src/cpu_2dp.cpp:243-260, src/cpu_3d.cpp:348-368,
+//                            src/cpu_3d.cpp:333-371
+//   * J layout / generation  src/cpu_2dp.cpp:243-260, src/cpu_3d.cpp:281-301,
 //                            GPU word assembly src/device_2d.cu:130-138,
 //                            src/device_3d.cu:98-125, src/device.cuh:4-8
 //   * draw schedule          src/random.cu:15-35, src/device_2d.cu:96-97
@@ -350,7 +350,7 @@ void sao_sys_init_J(void* p) {
     }
     o->draw += 2 * o->dim;
   } else {
-    // src/cpu_2dp.cpp:307-324, src/cpu_3d.cpp:348-368: one gen() per own word,
+    // src/cpu_2dp.cpp:243-260, src/cpu_3d.cpp:281-301: one gen() per own word,
     // site-major.
     for (long i = 0; i < o->N; ++i) {
       ox[i] = o->gen();
@@ -418,7 +418,7 @@ void sao_sys_measure(void* p, int64_t* E, int64_t* M) {
 
 // The reference's float vector, index j = replica bit j: the CPU classes add
 // bit_to_double(w, j) -- which tests bit 63-j of w (src/tools_inline.hpp:27-31)
-// -- into E[63-j] (src/cpu_2d.cpp:82-84, src/cpu_3d.cpp:413-415), so the two
+// -- into E[63-j] (src/cpu_2d.cpp:82-84, src/cpu_3d.cpp:346-348), so the two
 // reversals cancel.
 void sao_sys_measure_float(void* p, float* out64) {
   OSys* o = (OSys*)p;

@@ -3,10 +3,10 @@
 // colour-split lattice geometry.
 //
 // Reference semantics (paths relative to the reference project):
-//   bit logic   src/cpu_2d.cpp:5-41, src/cpu_2dp.cpp:336-383, src/cpu_3d.cpp:174-228,
+//   bit logic   src/cpu_2d.cpp:5-41, src/cpu_2dp.cpp:336-383, src/cpu_3d.cpp:107-161,
 //               src/device_2d.cu:53-87, src/device_3d.cu:246-292
 //   draws       src/random.cu:15-35, src/device_2d.cu:96-97
-//   colouring   src/cpu_2dp.cpp:106-114, src/cpu_3d.cpp:161-172: a site's colour
+//   colouring   src/cpu_2dp.cpp:106-114, src/cpu_3d.cpp:94-105: a site's colour
 //               is (x+y)%2 in 2D AND 3D, so in 3D the z neighbours share a
 //               colour and each half-sweep is sequential along z.
 #pragma once

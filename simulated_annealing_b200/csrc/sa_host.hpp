@@ -22,7 +22,7 @@ int cuda_fail(cudaError_t e, const char* what);
   } while (0)
 
 // Boltzmann table exactly as the reference builds it (double, glibc exp):
-// 2D src/cpu_2dp.cpp:33-40 (20 entries), 3D src/cpu_3d.cpp:99-104 (14 entries).
+// 2D src/cpu_2dp.cpp:33-40 (20 entries), 3D src/cpu_3d.cpp:218-232 (14 entries).
 void boltz_table(int lattice, double T, double h, double* out20);
 
 // u32 -> float in (0,1] used by the reference's per-site uniform draw; the

@@ -1,6 +1,6 @@
 // sa_measure.cuh -- block-level energy / magnetisation counting of one system
 // (the reference's measure(), src/cpu_2d.cpp:67-94, src/cpu_2dp.cpp:196-214,
-// src/cpu_3d.cpp:400-438, src/device_2d.cu:141-208), shared by the engine's
+// src/cpu_3d.cpp:333-371, src/device_2d.cu:141-208), shared by the engine's
 // measure kernels.
 #pragma once
 #include "sa_b200.h"

@@ -8,7 +8,7 @@
 // independent (one thread per site). In 3D the z neighbours share the colour,
 // so a thread walks one (x,y) column in increasing z, carrying the updated
 // spin of z-1 and the new z=0 spin for the periodic wrap -- exactly the order
-// of src/cpu_3d.cpp:161-172.
+// of src/cpu_3d.cpp:94-105.
 #include <cuda_runtime.h>
 
 #include <cstdio>
