@@ -278,20 +278,36 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
     ps.step(k * ns + sk);
     const int zsn = (yl > 0) ? zs : x.nyN * x.rowW;       // z stride of the north row's owner
     const int zss = (yl < x.ny - 1) ? zs : x.nyS * x.rowW;
-    int jo = y * hL + k, je = y * hL + ke, js = ys * hL + k;
+    const int jo = y * hL + k, je = y * hL + ke, js = ys * hL + k;
     SlotWords<SL> prev = {};
     if (valid) prev = ldw<SL>(x.sm + own + (L - 1) * zs);
     SlotWords<SL> first = {};
     for (int z0 = 0; z0 < L; z0 += P) {
+      // Lane (column cl, i) draws the Philox number and loads the six coupling
+      // words of plane z0+i; the column's P lanes share them by shuffles, so
+      // each coupling word is loaded once per site instead of once per slot.
       const int zd = z0 + (lane % P);
       uint32_t um = 0;
-      if (col_ok && zd < L)
+      word_t bw = 0, be = 0, bn = 0, bs = 0, bu = 0, bd = 0;
+      if (col_ok && zd < L) {
         um = philox_draw(x.seed, (unsigned long long)(xx + L * (y + L * zd)), draw);
+        const int zo = zd * zg;
+        bw = __ldg(Jxc + jo + zo);
+        be = __ldg(Jxo + je + zo);
+        bn = __ldg(Jyc + jo + zo);
+        bs = __ldg(Jyo + js + zo);
+        bu = __ldg(Jzc + jo + zo);
+        bd = __ldg(Jzc + jo + ((zd == L - 1) ? 0 : zo + zg));
+      }
 #pragma unroll 2
       for (int zi = 0; zi < P; ++zi) {
         const int z = z0 + zi;
         if (z >= L) break;  // warp-uniform
-        const uint32_t u = __shfl_sync(0xffffffffu, um, cl * P + zi);
+        const int src = cl * P + zi;
+        const uint32_t u = __shfl_sync(0xffffffffu, um, src);
+        const word_t jw = __shfl_sync(0xffffffffu, bw, src), je_ = __shfl_sync(0xffffffffu, be, src);
+        const word_t jn = __shfl_sync(0xffffffffu, bn, src), js_ = __shfl_sync(0xffffffffu, bs, src);
+        const word_t ju = __shfl_sync(0xffffffffu, bu, src), jd = __shfl_sync(0xffffffffu, bd, src);
         if (valid) {
           const bool last = (z == L - 1);
           const SlotWords<SL> si = ldw<SL>(x.sm + own);
@@ -300,9 +316,6 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
           const SlotWords<SL> se = ldw<SL>(x.sm + oe);
           const SlotWords<SL> sn = pn.template ld<SL>(0);
           const SlotWords<SL> ss = ps.template ld<SL>(0);
-          const word_t jw = __ldg(Jxc + jo), je_ = __ldg(Jxo + je), jn = __ldg(Jyc + jo);
-          const word_t js_ = __ldg(Jyo + js), ju = __ldg(Jzc + jo);
-          const word_t jd = __ldg(Jzc + (last ? jo - (L - 1) * zg : jo + zg));
           SlotWords<SL> nsw;
 #pragma unroll
           for (int q = 0; q < SL; ++q) {
@@ -322,9 +335,6 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         oe += zs;
         pn.step(zsn);
         ps.step(zss);
-        jo += zg;
-        je += zg;
-        js += zg;
       }
     }
   }
