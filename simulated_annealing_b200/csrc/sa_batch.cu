@@ -518,7 +518,8 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
         a = dc.pair;
         nsl = 2;
       }
-      rmeasure<CL>(x, d3, open, a, nsl, s_cnt);
+      if constexpr (P == 1 && SL == 1) rmeasure<CL, 4>(x, d3, open, a, nsl, s_cnt);
+      else rmeasure<CL>(x, d3, open, a, nsl, s_cnt);
       sync_all();
       if (threadIdx.x < 128) {
         unsigned v = 0;
@@ -866,6 +867,13 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
         int warps = std::min(passes, kResMaxWarps);
         const int rounds = (passes + warps - 1) / warps;
         warps = std::max(4, (passes + rounds - 1) / rounds);
+        if (d.nslots == 1 && smem >= 64 * 1024) {
+          // single-slot instances that occupy an SM alone are measured after
+          // every sweep: give the measurement pass (one unit = 32 sites of one
+          // colour and plane) at least ~4 units per warp of parallelism
+          const int units = 2 * ((d.lattice == SA_LATTICE_3D) ? d.L : 1) * ((ny * hL + 31) / 32);
+          warps = std::max(warps, std::min(kResMaxWarps, (units + 3) / 4));
+        }
         g.threads = warps * 32;
       }
       b->groups.push_back(g);

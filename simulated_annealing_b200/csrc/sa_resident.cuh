@@ -465,7 +465,9 @@ __device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw,
 
 // Partial satisfied-bond counts of slots a..a+nsl-1 over this CTA's sites
 // (each bond counted once, from its site towards -x/-y/-z) into cnt[q][j].
-template <bool CL>
+// UNR units are formed before any is added, so their loads are in flight
+// together (used where few warps walk many units: single-slot instances).
+template <bool CL, int UNR = 1>
 __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, int a, int nsl,
                                          unsigned (*cnt)[64]) {
   for (int i = threadIdx.x; i < 128; i += blockDim.x) (&cnt[0][0])[i] = 0;
@@ -479,45 +481,69 @@ __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, in
   VCount<16> big;
   sm4.clear();
   big.clear();
-  int it = 0;
   const int tiles = (cols + per - 1) / per;      // site tiles per (colour, z)
   const int units = 2 * x.zc * tiles;
   // warp w takes the contiguous units [u0, u1) and walks (cz, tile) without division
   const int u0 = (int)(((long)units * warp) / nwarps), u1 = (int)(((long)units * (warp + 1)) / nwarps);
   int cz = u0 / tiles, tile = u0 - cz * tiles;
-  for (int un = u0; un < u1; ++un) {
-    const int col = tile * per + g;
-    if (col < cols) {
-      const int c = (cz >= x.zc) ? 1 : 0, z = cz - c * x.zc;
-      const int yl = div_hl(col, x);
-      const int k = col - yl * hL, y = x.y0 + yl;
-      const int par = (c + y) & 1, xx = 2 * k + par;
-      int kw, ke;
-      x_neighbours(k, par, hL, kw, ke);
-      const int oc = 1 - c;
-      const int sk = slot ^ swz(x, k);
-      const word_t si = x.sm[lrow(x, c, z, yl) + k * ns + sk];
-      const long jr = (long)(y + L * z) * hL + k;
-      const word_t w = (open && xx == 0) ? 0 : (__ldg(x.J + (long)(0 + c) * x.half + jr) ^ si ^
-                                                 x.sm[lrow(x, oc, z, yl) + kw * ns + (slot ^ swz(x, kw))]);
-      const NbRow<CL> pn = north_row<CL>(x, oc, z, yl);
-      const word_t n = __ldg(x.J + (long)(2 + c) * x.half + jr) ^ si ^ pn.template ld<1>(k * ns + sk).w[0];
-      word_t q0, q1;
-      if (d3) {
-        const int zu = (z == 0) ? L - 1 : z - 1;
-        const word_t uu = __ldg(x.J + (long)(4 + c) * x.half + jr) ^ si ^ x.sm[lrow(x, c, zu, yl) + k * ns + sk];
-        q0 = w ^ n ^ uu;
-        q1 = (w & n) | (uu & (w ^ n));
-      } else {
-        q0 = w ^ n;
-        q1 = w & n;
-      }
-      add2_small(sm4, q0, q1);
+  // satisfied-bond bits (q1 q0 = 0..3) of this lane's site in unit (cz, tile)
+  auto unit_bits = [&](int cz_, int tile_, word_t& q0, word_t& q1) {
+    q0 = q1 = 0;
+    const int col = tile_ * per + g;
+    if (col >= cols) return;
+    const int c = (cz_ >= x.zc) ? 1 : 0, z = cz_ - c * x.zc;
+    const int yl = div_hl(col, x);
+    const int k = col - yl * hL, y = x.y0 + yl;
+    const int par = (c + y) & 1, xx = 2 * k + par;
+    int kw, ke;
+    x_neighbours(k, par, hL, kw, ke);
+    const int oc = 1 - c;
+    const int sk = slot ^ swz(x, k);
+    const word_t si = x.sm[lrow(x, c, z, yl) + k * ns + sk];
+    const long jr = (long)(y + L * z) * hL + k;
+    const word_t w = (open && xx == 0) ? 0 : (__ldg(x.J + (long)(0 + c) * x.half + jr) ^ si ^
+                                               x.sm[lrow(x, oc, z, yl) + kw * ns + (slot ^ swz(x, kw))]);
+    const NbRow<CL> pn = north_row<CL>(x, oc, z, yl);
+    const word_t n = __ldg(x.J + (long)(2 + c) * x.half + jr) ^ si ^ pn.template ld<1>(k * ns + sk).w[0];
+    if (d3) {
+      const int zu = (z == 0) ? L - 1 : z - 1;
+      const word_t uu = __ldg(x.J + (long)(4 + c) * x.half + jr) ^ si ^ x.sm[lrow(x, c, zu, yl) + k * ns + sk];
+      q0 = w ^ n ^ uu;
+      q1 = (w & n) | (uu & (w ^ n));
+    } else {
+      q0 = w ^ n;
+      q1 = w & n;
     }
+  };
+  auto advance = [&]() {
     if (++tile == tiles) {
       tile = 0;
       ++cz;
     }
+  };
+  int un = u0;
+  if (UNR > 1) {
+    // UNR <= 5 units of <= 3 bonds per round keep the small counter below 16
+    static_assert(UNR <= 5, "small counter range");
+    for (; un + UNR <= u1; un += UNR) {
+      word_t b0[UNR], b1[UNR];
+#pragma unroll
+      for (int i = 0; i < UNR; ++i) {
+        unit_bits(cz, tile, b0[i], b1[i]);
+        advance();
+      }
+#pragma unroll
+      for (int i = 0; i < UNR; ++i) add2_small(sm4, b0[i], b1[i]);
+      add_small(big, sm4);
+      sm4.clear();
+    }
+  }
+  int it = 0;
+  for (; un < u1; ++un) {
+    word_t b0, b1;
+    unit_bits(cz, tile, b0, b1);
+    add2_small(sm4, b0, b1);
+    advance();
     if (++it == 5) {
       add_small(big, sm4);
       sm4.clear();
