@@ -34,8 +34,10 @@ serving    continuous batching of anneal requests (simulated_annealing_b200.serv
            [1e3, 1e5], linear T 3.0 -> 0.2 in steps of 100 sweeps, couplings and
            spins from per-request seeds; p50/p99 time from arrival to result on
            the host clock and aggregate attempts/ns. The default run serves the
-           first --serve-requests requests of that stream; --workload serve runs
-           the whole 20,000.
+           first --serve-requests (300) requests of that stream at 2,000/s and
+           the first half of them at --serve-sustainable-rate (30/s), a rate the
+           GPU keeps up with; --workload serve runs the whole 20,000 (or
+           --serve-requests) at --serve-rate.
 
 --workload c1|c2|c3 time the single-lattice cases instead (2D L=64 T=1.0 for
 10,000 sweeps; 3D L=32 anneal 3.0 -> 0.2 over 200 x 100 sweeps; 3D L=16
@@ -415,6 +417,10 @@ def run_ours(args):
             line["batched_over_plain"] = value / pl["value"]
         if world == 1 and args.serve_requests > 0:
             line["serving"] = serving_run(args.serve_requests, 2000.0, args.serve_budget_gb)
+            # the same stream at an arrival rate the GPU sustains (arrivals spread
+            # over ~5 s instead of queueing up at once)
+            line["serving_sustainable"] = serving_run(args.serve_requests // 2, args.serve_sustainable_rate,
+                                                      args.serve_budget_gb)
         print(json.dumps(line), flush=True)
     b.close()
     if dist:
@@ -459,9 +465,12 @@ def run_single(args):
             "vs_baseline": None, "dtype": "u64 (bitwise/int32)", "data": "synthetic"}
     if args.workload == "serve":
         clocks.start()
-        r = serving_run(20_000, 2000.0, 120.0)
+        n = args.serve_requests if args.serve_requests else 20_000
+        r = serving_run(n, args.serve_rate, min(120.0, args.serve_budget_gb))
         line = dict(base, metric="anneal time-to-result p99 (s)", value=r["p99_s"], unit="s",
-                    higher_is_better=False, config={"workload": "serving: 20,000 anneal requests, Poisson 2,000/s"},
+                    higher_is_better=False,
+                    config={"workload": f"serving: the first {n} anneal requests of the stream, Poisson "
+                                        f"{args.serve_rate:g}/s"},
                     serving=r)
         line["clocks"] = clocks.stop()
         print(json.dumps(line), flush=True)
@@ -536,10 +545,16 @@ def main():
     ap.add_argument("--ref-step-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-budget", type=float, default=8.0, help="seconds of the plain form (0 = skip)")
-    ap.add_argument("--serve-requests", type=int, default=300, help="requests in the serving sample (0 = skip)")
+    ap.add_argument("--serve-requests", type=int, default=None,
+                    help="requests in the serving sample (0 = skip; default 300, or 20,000 for --workload serve)")
     ap.add_argument("--serve-budget-gb", type=float, default=16.0)
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="arrivals/s of --workload serve")
+    ap.add_argument("--serve-sustainable-rate", type=float, default=30.0,
+                    help="arrivals/s of the default line's second serving sample")
     ap.add_argument("--workload", choices=["c4", "serve", "c1", "c2", "c3"], default="c4")
     args = ap.parse_args()
+    if args.serve_requests is None and args.workload == "c4":
+        args.serve_requests = 300
     if args.workload != "c4" and args.impl == "ours":
         return run_single(args)
     if args.warmup < 3 and args.impl == "ours":
