@@ -809,10 +809,34 @@ static int batch_params(sa_batch* b, long nsweeps, BatchParams* p) {
 
 // Work order and launch groups of the current instance table: grouped by
 // (kernel, lanes-per-site, cluster size, shape), most expensive first.
+// A batch whose smallest clusters leave SMs idle (a few large instances: one
+// PT ensemble, the last requests of a serving run) gets larger clusters, so
+// each instance's rows are shared by more SMs: every cluster size is scaled by
+// the idle factor, up to 16 CTAs and one y-row per CTA.
+static void spread_clusters(sa_batch* b) {
+  static const int cands[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  long total = 0;
+  for (int C : b->cluster_of) total += C;
+  if (total == 0 || total * 2 > sms) return;
+  const long factor = sms / total;
+  for (size_t i = 0; i < b->inst.size(); ++i) {
+    const int C0 = b->cluster_of[i];
+    if (C0 == 0) continue;
+    const long want = std::min<long>((long)C0 * factor, std::min(16, b->inst[i].L));
+    int best = C0;
+    for (int C : cands)
+      if (C <= want && C > best) best = C;
+    b->cluster_of[i] = best;
+  }
+}
+
 static std::vector<int32_t> build_groups(sa_batch* b) {
   // work order: grouped by (kernel, P, C), most expensive first inside a group
   b->cluster_of.resize(b->inst.size());
   for (size_t i = 0; i < b->inst.size(); ++i) b->cluster_of[i] = b->force_global ? 0 : choose_cluster(b->inst[i]);
+  spread_clusters(b);
   std::vector<int32_t> order(b->inst.size());
   for (size_t i = 0; i < order.size(); ++i) order[i] = (int32_t)i;
   std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
