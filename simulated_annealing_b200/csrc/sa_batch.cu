@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
     }
     for (int c = 0; c < 2; ++c) {
       if (d3) {
-        if (P == 1 && SL == 1 && x.L > 4) rhalf_3d1<4, CL>(x, c, draw + c, th[0]);
+        if (P == 1 && SL == 1 && x.L > 4) rhalf_3d1<2, CL>(x, c, draw + c, th[0]);
         else rhalf_3d<P, SL, CL>(x, c, draw + c, th);
       }
       else rhalf_2d<P, SL, open, CL>(x, c, draw + c, th, tb);

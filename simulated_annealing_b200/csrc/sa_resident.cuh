@@ -304,10 +304,14 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         const int z = z0 + zi;
         if (z >= L) break;  // warp-uniform
         const int src = cl * P + zi;
-        const uint32_t u = __shfl_sync(0xffffffffu, um, src);
-        const word_t jw = __shfl_sync(0xffffffffu, bw, src), je_ = __shfl_sync(0xffffffffu, be, src);
-        const word_t jn = __shfl_sync(0xffffffffu, bn, src), js_ = __shfl_sync(0xffffffffu, bs, src);
-        const word_t ju = __shfl_sync(0xffffffffu, bu, src), jd = __shfl_sync(0xffffffffu, bd, src);
+        // one lane per site (P = 1): the lane's own draw and couplings
+        const uint32_t u = (P == 1) ? um : __shfl_sync(0xffffffffu, um, src);
+        const word_t jw = (P == 1) ? bw : __shfl_sync(0xffffffffu, bw, src);
+        const word_t je_ = (P == 1) ? be : __shfl_sync(0xffffffffu, be, src);
+        const word_t jn = (P == 1) ? bn : __shfl_sync(0xffffffffu, bn, src);
+        const word_t js_ = (P == 1) ? bs : __shfl_sync(0xffffffffu, bs, src);
+        const word_t ju = (P == 1) ? bu : __shfl_sync(0xffffffffu, bu, src);
+        const word_t jd = (P == 1) ? bd : __shfl_sync(0xffffffffu, bd, src);
         if (valid) {
           const bool last = (z == L - 1);
           const SlotWords<SL> si = ldw<SL>(x.sm + own);
