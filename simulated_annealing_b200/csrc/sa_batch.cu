@@ -33,6 +33,7 @@
 #include "sa_device.cuh"
 #include "sa_host.hpp"
 #include "sa_resident.cuh"
+#include "sa_system.hpp"
 
 namespace sa {
 
@@ -569,6 +570,10 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
       sync_all();
       if (meas) measured += 1;
     }
+    if (p.step_rec && d.sched >= 0 && q == 0 && threadIdx.x < 64 && sweeps % d.sweeps_per_step == 0) {
+      const int64_t stp = sweeps / d.sweeps_per_step - 1;
+      if (stp < d.thr_count) p.step_rec[((int64_t)d.state_idx * d.thr_count + stp) * 64 + threadIdx.x] = my_elast;
+    }
   }
   // local -> global
   for (int cz = 0; cz < 2 * x.zc; ++cz) {
@@ -804,6 +809,7 @@ static int batch_params(sa_batch* b, long nsweeps, BatchParams* p) {
   p->mstride = b->mstride;
   p->hist = b->d_hist;
   p->hstride = b->hstride > 0 ? b->hstride : 1;
+  p->step_rec = nullptr;
   return SA_OK;
 }
 
@@ -2011,3 +2017,122 @@ int sa_serve_active(sa_serve_t s, int* n, long long* free_words) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// One lattice of a single system (sa_system: spins [colour][row][k] and
+// couplings [axis][colour][row][k], the batch layout with one slot) run by the
+// resident kernel: the whole schedule in one launch, the lattice in the shared
+// memory of a cluster spread over up to 16 SMs. Zero field only (the batch
+// threshold tables have no field term).
+// ===========================================================================
+namespace sa {
+
+bool resident_ok(const sa_system* sy) {
+  return sy->h == 0.0 && sy->L >= 4 && sy->N <= kBatchMaxN;
+}
+
+int resident_run(sa_system* sy, const double* T, int nsteps, int sweeps, int stride, int64_t* Emax,
+                 int64_t* step_E, int* measured) {
+  if (!resident_ok(sy)) return fail(SA_ERR_UNSUPPORTED, "lattice not supported by the resident runner");
+  if (nsteps < 1 || sweeps < 1 || stride < 0) return fail(SA_ERR_INVALID, "bad schedule");
+  std::vector<BThr> thr(nsteps);
+  for (int k = 0; k < nsteps; ++k) {
+    if (!(T[k] > 0)) return fail(SA_ERR_INVALID, "temperatures must be > 0");
+    thr[k] = to_bthr(sy->lattice, T[k]);
+  }
+  sa_batch tmp;
+  tmp.device = sy->device;
+  tmp.stream = sy->stream;
+  InstDesc d;
+  memset(&d, 0, sizeof d);
+  d.lattice = sy->lattice;
+  d.L = sy->L;
+  d.nslots = 1;
+  d.P = 1;
+  d.ladder = -1;
+  d.sched = 0;
+  d.sweeps_per_step = sweeps;
+  d.thr_count = nsteps;
+  d.N = sy->N;
+  d.half = sy->half;
+  d.nbonds = sy->nbonds;
+  d.hist_off = -1;
+  d.seed = sy->seed;
+  d.sweep_limit = (int64_t)nsteps * sweeps;
+  tmp.inst.push_back(d);
+  std::vector<int32_t> order = build_groups(&tmp);
+  if (tmp.groups.size() != 1 || !tmp.groups[0].resident)
+    return fail(SA_ERR_UNSUPPORTED, "lattice does not fit a cluster's shared memory");
+  // one device block: descriptor, state, order, work counter, pair counters,
+  // thresholds, per-step record
+  const size_t o_state = 256, o_order = o_state + ((sizeof(InstState) + 255) / 256) * 256;
+  const size_t o_work = o_order + 256, o_acc = o_work + 256, o_thr = o_acc + 256;
+  const size_t o_rec = o_thr + ((nsteps * sizeof(BThr) + 255) / 256) * 256;
+  const size_t bytes = o_rec + (size_t)nsteps * 64 * sizeof(int64_t);
+  char* blk = nullptr;
+  SA_CUDA_TRY(cudaMalloc(&blk, bytes));
+  auto release = [&]() { cudaFree(blk); };
+  InstState st;
+  memset(&st, 0, sizeof st);
+  st.draw = sy->draw;
+  tmp.d_inst = reinterpret_cast<InstDesc*>(blk);
+  tmp.d_state = reinterpret_cast<InstState*>(blk + o_state);
+  tmp.d_order = reinterpret_cast<int32_t*>(blk + o_order);
+  tmp.d_work = reinterpret_cast<int32_t*>(blk + o_work);
+  tmp.d_acc = reinterpret_cast<int64_t*>(blk + o_acc);
+  tmp.d_att = tmp.d_acc + 1;
+  tmp.d_thr = reinterpret_cast<BThr*>(blk + o_thr);
+  tmp.d_spins = sy->d_s;
+  tmp.d_J = sy->d_J;
+  tmp.mstride = stride;
+  int64_t* d_rec = reinterpret_cast<int64_t*>(blk + o_rec);
+  cudaError_t e = cudaMemcpyAsync(tmp.d_inst, &d, sizeof d, cudaMemcpyHostToDevice, sy->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tmp.d_state, &st, sizeof st, cudaMemcpyHostToDevice, sy->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tmp.d_order, order.data(), sizeof(int32_t), cudaMemcpyHostToDevice, sy->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(tmp.d_work, 0, 256 + 256, sy->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tmp.d_thr, thr.data(), nsteps * sizeof(BThr), cudaMemcpyHostToDevice, sy->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_rec, 0, (size_t)nsteps * 64 * sizeof(int64_t), sy->stream);
+  if (e != cudaSuccess) {
+    release();
+    return cuda_fail(e, "resident_run set-up");
+  }
+  sa_batch::Group& g = tmp.groups[0];
+  g.stream = sy->stream;
+  int mc = 0;
+  int status = dispatch(&tmp, g, 0, 0, 2, &mc);
+  if (status == SA_OK) {
+    BatchParams prm;
+    batch_params(&tmp, d.sweep_limit, &prm);
+    prm.order = tmp.d_order;
+    prm.ninst = 1;
+    prm.work = tmp.d_work;
+    prm.step_rec = d_rec;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)g.C, 1, 1);
+    cfg.blockDim = dim3((unsigned)g.threads, 1, 1);
+    cfg.dynamicSmemBytes = g.smem;
+    cfg.stream = sy->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)g.C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void (*kern)(BatchParams) = resident_kernel<1>(g);
+    e = cudaLaunchKernelEx(&cfg, kern, prm);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&st, tmp.d_state, sizeof st, cudaMemcpyDeviceToHost, sy->stream);
+    if (e == cudaSuccess && step_E)
+      e = cudaMemcpyAsync(step_E, d_rec, (size_t)nsteps * 64 * sizeof(int64_t), cudaMemcpyDeviceToHost, sy->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sy->stream);
+    if (e != cudaSuccess) status = cuda_fail(e, "resident_run");
+  }
+  release();
+  if (status != SA_OK) return status;
+  if (Emax) memcpy(Emax, st.emax, sizeof st.emax);
+  if (measured) *measured = (int)st.measured;
+  sy->draw = st.draw;
+  return SA_OK;
+}
+
+}  // namespace sa

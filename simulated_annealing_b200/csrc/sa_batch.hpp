@@ -64,6 +64,8 @@ struct BatchParams {
   int32_t mstride;         // anneal measure stride (0 = never)
   int32_t* hist;           // energy histograms (bin (E+nbonds)/2), or null
   int32_t hstride;         // histogram every hstride sweeps
+  int64_t* step_rec;       // anneal: last measured -H at the end of every step
+                           // [state][step][64], or null
 };
 
 }  // namespace sa

@@ -167,6 +167,17 @@ extern "C" int sa_sys_anneal(sa_system_t sy, const double* T, int nsteps, int sw
     if (!(T[k] > 0)) return fail(SA_ERR_INVALID, "temperatures must be > 0");
     if (!make_thresholds(sy->lattice, T[k], sy->h, &thr[k])) return fail(SA_ERR_INVALID, "non-monotone table");
   }
+  if (resident_ok(sy)) {
+    // zero field: the whole schedule in one launch of the resident kernel
+    int64_t emax[64];
+    int measured = 0;
+    const int st = resident_run(sy, T, nsteps, sweeps, stride, emax, step_E, &measured);
+    if (st != SA_OK) return st;
+    for (int j = 0; j < 64; ++j) min_E[j] = measured ? (float)emax[j] : 0.f;
+    sy->T = T[nsteps - 1];
+    sy->thr = thr[nsteps - 1];
+    return SA_OK;
+  }
   Thresholds* d_thr = nullptr;
   AnnealState* d_st = nullptr;
   int64_t* d_stepE = nullptr;

@@ -262,6 +262,11 @@ int launch_measure(sa_system* sy, int64_t* d_E, int64_t* d_M) {
 
 using namespace sa;
 
+// Sweep counts from which sa_sys_sweep hands a zero-field lattice to the
+// resident kernel (one launch, lattice held in shared memory) instead of two
+// launches per sweep.
+static constexpr long kResidentMinSweeps = 16;
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -496,6 +501,11 @@ int sa_sys_get_J(sa_system_t sy, uint64_t* jx, uint64_t* jy, uint64_t* jz) {
 int sa_sys_sweep(sa_system_t sy, long nsweeps) {
   if (!sy) return fail(SA_ERR_INVALID, "null system");
   if (nsweeps < 0) return fail(SA_ERR_INVALID, "nsweeps < 0");
+  if (nsweeps >= kResidentMinSweeps && nsweeps <= 0x7FFFFFFF && resident_ok(sy)) {
+    // long runs at zero field: one launch of the resident kernel
+    const double T = sy->T;
+    return resident_run(sy, &T, 1, (int)nsweeps, 0, nullptr, nullptr, nullptr);
+  }
   for (long k = 0; k < nsweeps; ++k) {
     launch_halfsweep(sy, 0, sy->draw);
     launch_halfsweep(sy, 1, sy->draw + 1);

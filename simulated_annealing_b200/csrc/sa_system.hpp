@@ -22,4 +22,12 @@ struct sa_system {
 namespace sa {
 int launch_halfsweep(sa_system* sy, int c, unsigned long long draw);
 int launch_measure(sa_system* sy, int64_t* d_E, int64_t* d_M);
+// The shared-memory-resident batch kernel applied to one system (zero field,
+// L >= 4): nsteps steps of `sweeps` sweeps at T[k], -H measured every `stride`
+// sweeps of a step (0 = never). Host outputs, each may be null: Emax[64]
+// (running max of -H), step_E[nsteps*64] (last measurement of every step),
+// *measured (measurements taken). Advances the system's draw counter.
+bool resident_ok(const sa_system* sy);
+int resident_run(sa_system* sy, const double* T, int nsteps, int sweeps, int stride, int64_t* Emax,
+                 int64_t* step_E, int* measured);
 }  // namespace sa

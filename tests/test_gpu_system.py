@@ -54,6 +54,25 @@ def test_sweeps_bit_exact(sab, lat, L, T, h):
     assert g.rng_state()[1] == o.draw
 
 
+@pytest.mark.parametrize("lat,L", [(lat, L) for lat, L in LATS if L >= 4])
+def test_long_sweeps_resident_path(sab, lat, L):
+    """Zero-field runs of >= 16 sweeps go through the shared-memory-resident
+    kernel (one launch); short runs keep two launches per sweep. Alternating
+    them must follow the oracle draw for draw."""
+    g, o = _pair(sab, lat, L, 0.9)
+    _setup((g, o), 7, 8)
+    for n in (40, 3, 17, 1, 64):
+        g.sweep(n)
+        o.sweep(n)
+        _check(g, o)
+    assert g.rng_state()[1] == o.draw
+    g.set_T(2.3)
+    o.set_T(2.3)
+    g.sweep(25)
+    o.sweep(25)
+    _check(g, o)
+
+
 def test_init_J_without_reset_consumes_draws(sab):
     # timing-mode flow (src/main_gpu.cu:165-166): init_J then sweeps continue at draw t
     g, o = _pair(sab, O.LAT_3D, 6, 0.8)
