@@ -51,6 +51,12 @@ enum {
   SA_LATTICE_3D = 2         /* cpu_3d / gpu_3d: cubic, periodic */
 };
 
+/* Random-number modes (sa_sys_set_rng_mode). */
+enum {
+  SA_RNG_PHILOX = 0,     /* the GPU reference's cuRAND Philox schedule (default) */
+  SA_RNG_MT19937_64 = 1  /* the CPU reference's std::mt19937_64 stream */
+};
+
 typedef struct sa_system* sa_system_t;
 
 /* Last error message of the calling thread ("" if none). */
@@ -107,6 +113,21 @@ int sa_sys_measure_async(sa_system_t sys, int64_t* d_E, int64_t* d_M);
 int sa_sys_swap(sa_system_t a, sa_system_t b, uint64_t mask);
 /* get_N: src/gpu_2d.cu:301-303. */
 int sa_sys_get_N(sa_system_t sys, long* N);
+/* Random-number source of a system.
+ * SA_RNG_PHILOX (default): the GPU reference's schedule, cuRAND Philox4x32-10
+ *   with key = seed and subsequence = site (src/random.cu:15-35), one draw per
+ *   site per half-sweep (src/device_2d.cu:96-97).
+ * SA_RNG_MT19937_64: the CPU reference's stream, one std::mt19937_64 per system
+ *   (src/cpu_2dp.hpp:35-36, src/cpu_3d.hpp:37-39) generated on the device and
+ *   consumed as cpu_2d / cpu_2dp / cpu_3d consume it: set_seed reseeds it
+ *   (src/cpu_3d.cpp:210), init_J takes dim*N outputs (src/cpu_2dp.cpp:243-260,
+ *   src/cpu_3d.cpp:281-301), init_rand N (src/cpu_3d.cpp:257-263), and a sweep
+ *   one uniform_real_distribution<double> draw per site in the reference's
+ *   visiting order (src/cpu_3d.cpp:94-105, :130). Spins, couplings and
+ *   energies then match the unmodified reference CPU classes bit for bit.
+ *   Switching to it reseeds the generator with the current seed. */
+int sa_sys_set_rng_mode(sa_system_t sys, int mode);
+int sa_sys_get_rng_mode(sa_system_t sys, int* mode);
 /* RNG position (for checkpoints): draw counter and spin-init epoch. */
 int sa_sys_get_rng(sa_system_t sys, uint64_t* seed, uint64_t* draw, uint64_t* epoch);
 int sa_sys_set_rng(sa_system_t sys, uint64_t seed, uint64_t draw, uint64_t epoch);

@@ -127,6 +127,9 @@ class b200_sys : public gpu_sys {
   }
 
   // not part of gpu_sys
+  // SA_RNG_MT19937_64: draw from the CPU reference's std::mt19937_64 stream,
+  // so results match cpu_2d / cpu_2dp / cpu_3d bit for bit (sa_b200.h).
+  void set_rng_mode(int mode) { report(sa_sys_set_rng_mode(sys_, mode), "set_rng_mode"); }
   sa_system_t handle() const { return sys_; }
   int lattice() const { return lattice_; }
   void get_spins(uint64_t* s) { report(sa_sys_get_spins(sys_, s), "get_spins"); }

@@ -27,6 +27,7 @@ SA_ERR_UNSUPPORTED = 10
 SA_LATTICE_2D = 0
 SA_LATTICE_2D_OPEN_X = 1
 SA_LATTICE_3D = 2
+SA_RNG_PHILOX, SA_RNG_MT19937_64 = 0, 1
 
 
 class SAError(RuntimeError):
@@ -72,6 +73,8 @@ _PROTOS = {
     "sa_sys_swap": (_c.c_int, [_vp, _vp, _u64]),
     "sa_sys_get_N": (_c.c_int, [_vp, _c.POINTER(_c.c_long)]),
     "sa_sys_get_rng": (_c.c_int, [_vp, _u64p, _u64p, _u64p]),
+    "sa_sys_set_rng_mode": (_c.c_int, [_vp, _c.c_int]),
+    "sa_sys_get_rng_mode": (_c.c_int, [_vp, _c.POINTER(_c.c_int)]),
     "sa_sys_set_rng": (_c.c_int, [_vp, _u64, _u64, _u64]),
     "sa_sys_sync": (_c.c_int, [_vp]),
     "sa_sys_save": (_c.c_int, [_vp, _vp, _c.c_size_t, _szp]),

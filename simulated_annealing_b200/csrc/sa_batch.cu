@@ -2028,7 +2028,7 @@ int sa_serve_active(sa_serve_t s, int* n, long long* free_words) {
 namespace sa {
 
 bool resident_ok(const sa_system* sy) {
-  return sy->h == 0.0 && sy->L >= 4 && sy->N <= kBatchMaxN;
+  return sy->rng_mode == SA_RNG_PHILOX && sy->h == 0.0 && sy->L >= 4 && sy->N <= kBatchMaxN;
 }
 
 int resident_run(sa_system* sy, const double* T, int nsteps, int sweeps, int stride, int64_t* Emax,

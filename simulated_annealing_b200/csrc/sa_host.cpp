@@ -93,6 +93,72 @@ bool make_thresholds(int lattice, double T, double h, Thresholds* t) {
   return true;
 }
 
+double uniform_from_u64(uint64_t g) {
+  // generate_canonical<double, 53> with a 64-bit engine: one draw scaled by
+  // 2^-64; a result that rounds up to 1 is replaced by the largest double < 1
+  volatile double d = (double)g;
+  volatile double r = d * 0x1p-64;
+  return r >= 1.0 ? 0x1.fffffffffffffp-1 : r;
+}
+
+// Largest g with u(g) < b (b > 0; u(0) = 0 < b).
+static uint64_t threshold_mt(double b) {
+  // smallest g in [0, 2^64] with u(g) >= b, by bisection on 128-bit bounds
+  unsigned __int128 lo = 0, hi = (unsigned __int128)1 << 64;
+  while (lo < hi) {
+    const unsigned __int128 mid = (lo + hi) >> 1;
+    if (uniform_from_u64((uint64_t)mid) < b) lo = mid + 1;
+    else hi = mid;
+  }
+  return (uint64_t)(lo - 1);  // lo >= 1 since u(0) = 0 < b
+}
+
+bool make_thresholds_mt(int lattice, double T, double h, ThresholdsMT* t) {
+  double b[20];
+  boltz_table(lattice, T, h, b);
+  memset(t, 0, sizeof *t);
+  const int nb = (lattice == SA_LATTICE_3D) ? 6 : 4;
+  const int up0 = nb + 1;
+  // entries accepting something (b > 0) must form a prefix of each table
+  auto fill = [&](const double* bt, int n, uint64_t* thr, int* nvalid) {
+    *nvalid = 0;
+    for (int k = 0; k < n; ++k) {
+      if (bt[k] > 0) {
+        if (*nvalid != k) return false;
+        thr[k] = threshold_mt(bt[k]);
+        *nvalid = k + 1;
+      }
+    }
+    return true;
+  };
+  if (!fill(b, nb + 1, t->dn, &t->ndn) || !fill(b + up0, nb + 1, t->up, &t->nup)) return false;
+  if (lattice != SA_LATTICE_3D) {
+    // entry 0 of the border tables (0 in the reference) is never consulted: a
+    // border site's forced bond is satisfied; entry 1 stands in for it
+    double bb[5], bu[5];
+    for (int k = 0; k <= 4; ++k) {
+      bb[k] = b[10 + (k == 0 ? 1 : k)];
+      bu[k] = b[15 + (k == 0 ? 1 : k)];
+    }
+    if (!fill(bb, 5, t->bdn, &t->nbdn) || !fill(bu, 5, t->bup, &t->nbup)) return false;
+  }
+  for (int k = 1; k < t->ndn; ++k)
+    if (t->dn[k] > t->dn[k - 1]) return false;
+  for (int k = 1; k < t->nup; ++k)
+    if (t->up[k] > t->up[k - 1]) return false;
+  for (int k = 1; k < t->nbdn; ++k)
+    if (t->bdn[k] > t->bdn[k - 1]) return false;
+  for (int k = 1; k < t->nbup; ++k)
+    if (t->bup[k] > t->bup[k - 1]) return false;
+  return true;
+}
+
+void mt64_seed(uint64_t seed, uint64_t* st) {
+  st[0] = seed;
+  for (int i = 1; i < kMtN; ++i) st[i] = 6364136223846793005ULL * (st[i - 1] ^ (st[i - 1] >> 62)) + (uint64_t)i;
+  st[kMtN] = kMtN;
+}
+
 bool pt_accept(float dE, double dB, double r) {
   return ((dE * dB) > 0.) || r < exp(dB * dE);
 }

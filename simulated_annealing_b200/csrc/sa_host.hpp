@@ -34,6 +34,12 @@ uint32_t threshold_of(float b);
 // Integer thresholds of a lattice at (T, h): float-cast table, then thr().
 // Returns false if the table is not monotone where the kernels need it.
 bool make_thresholds(int lattice, double T, double h, Thresholds* out);
+// Tables for the mt19937_64 stream (see ThresholdsMT).
+bool make_thresholds_mt(int lattice, double T, double h, ThresholdsMT* out);
+// The reference CPU classes' uniform: u(g) for a 64-bit generator output.
+double uniform_from_u64(uint64_t g);
+// mt19937_64 seeding (state words then index kMtN: the next output twists).
+void mt64_seed(uint64_t seed, uint64_t* state313);
 
 // Exchange decision of src/parallel_tempering.hpp:141-162 for one replica:
 // accept iff (dE*dB > 0) || r < exp(dB*dE), dE = -(E_i - E_{i+1}) as float.

@@ -9,6 +9,7 @@
 // captured once as a CUDA graph and replayed for every step.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -166,6 +167,34 @@ extern "C" int sa_sys_anneal(sa_system_t sy, const double* T, int nsteps, int sw
   for (int k = 0; k < nsteps; ++k) {
     if (!(T[k] > 0)) return fail(SA_ERR_INVALID, "temperatures must be > 0");
     if (!make_thresholds(sy->lattice, T[k], sy->h, &thr[k])) return fail(SA_ERR_INVALID, "non-monotone table");
+  }
+  if (sy->rng_mode == SA_RNG_MT19937_64) {
+    // the CPU reference's stream: annealing<>'s own loop (src/annealing.hpp:67-100)
+    // over sa_sys_sweep / sa_sys_measure, which draw from the device generator
+    std::vector<double> mn(64, 0.0);
+    std::vector<int64_t> last(64, 0);
+    int measured = 0;
+    for (int k = 0; k < nsteps; ++k) {
+      int st = sa_sys_set_T(sy, T[k]);
+      for (int i = 0; st == SA_OK && i < sweeps; ++i) {
+        st = sa_sys_sweep(sy, 1);
+        if (st == SA_OK && stride != 0 && i % stride == 0) {
+          int64_t E[64], M[64];
+          st = sa_sys_measure(sy, E, M);
+          for (int j = 0; st == SA_OK && j < 64; ++j) {
+            const double v = (double)(float)((double)E[j] + sy->h * (double)M[j]);
+            mn[j] = measured ? std::max(mn[j], v) : v;
+            last[j] = E[j];
+          }
+          if (st == SA_OK) ++measured;
+        }
+      }
+      if (st != SA_OK) return st;
+      if (step_E) memcpy(step_E + (long)k * 64, last.data(), 64 * sizeof(int64_t));
+    }
+    for (int j = 0; j < 64; ++j) min_E[j] = measured ? (float)mn[j] : 0.f;
+    sy->thr = thr[nsteps - 1];
+    return SA_OK;
   }
   if (resident_ok(sy)) {
     // zero field: the whole schedule in one launch of the resident kernel

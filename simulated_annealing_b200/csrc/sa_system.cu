@@ -30,12 +30,24 @@ namespace sa {
 // ---------------------------------------------------------------------------
 
 // One 2D half-sweep of colour c; one thread per site of that colour.
-template <bool OPEN_X>
+// Prefix t(g) = #{k < n : g <= thr[k]} of an mt19937_64 table (ThresholdsMT).
+template <int NB>
+__device__ __forceinline__ uint32_t prefix_count_mt(uint64_t g, const uint64_t* thr, int n) {
+  uint32_t t = 0;
+#pragma unroll
+  for (int k = 0; k <= NB; ++k) t += (k < n && g <= thr[k]) ? 1u : 0u;
+  return t;
+}
+
+// MT: the site's draw is the pass's mt19937_64 output at its rank in the
+// reference's sweep order (draws[idx], idx = row * L/2 + k), not Philox.
+template <bool OPEN_X, bool MT = false>
 __global__ void __launch_bounds__(256) k_halfsweep_2d(word_t* __restrict__ s,
                                                       const word_t* __restrict__ J, int L,
                                                       unsigned long long seed,
                                                       unsigned long long draw, int c,
-                                                      Thresholds thr) {
+                                                      Thresholds thr, const uint64_t* __restrict__ draws = nullptr,
+                                                      ThresholdsMT tm = {}) {
   const int hL = L >> 1;
   const long half = (long)L * hL;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -63,27 +75,40 @@ __global__ void __launch_bounds__(256) k_halfsweep_2d(word_t* __restrict__ s,
     if (x == 0) { mw = ~0ULL; border = true; }
     if (x == L - 1) { me = ~0ULL; border = true; }
   }
-  const unsigned long long site = (unsigned long long)x + (unsigned long long)L * y;
-  uint32_t u = philox_draw(seed, site, draw);
   word_t c0, c1, c2;
   count4(mw, me, mn, ms, c0, c1, c2);
   uint32_t tdn, tup;
-  if (OPEN_X && border) {
-    tdn = prefix_count<4>(u, thr.bdn);
-    tup = prefix_count<4>(u, thr.bup);
+  if (MT) {
+    const uint64_t g = draws[idx];
+    if (OPEN_X && border) {
+      tdn = prefix_count_mt<4>(g, tm.bdn, tm.nbdn);
+      tup = prefix_count_mt<4>(g, tm.bup, tm.nbup);
+    } else {
+      tdn = prefix_count_mt<4>(g, tm.dn, tm.ndn);
+      tup = prefix_count_mt<4>(g, tm.up, tm.nup);
+    }
   } else {
-    tdn = prefix_count<4>(u, thr.dn);
-    tup = prefix_count<4>(u, thr.up);
+    const unsigned long long site = (unsigned long long)x + (unsigned long long)L * y;
+    const uint32_t u = philox_draw(seed, site, draw);
+    if (OPEN_X && border) {
+      tdn = prefix_count<4>(u, thr.bdn);
+      tup = prefix_count<4>(u, thr.bup);
+    } else {
+      tdn = prefix_count<4>(u, thr.dn);
+      tup = prefix_count<4>(u, thr.up);
+    }
   }
   sc[idx] = flip_word(si, c0, c1, c2, tdn, tup);
 }
 
 // One 3D half-sweep of colour c; one thread per (x,y) column, walking z.
+template <bool MT = false>
 __global__ void __launch_bounds__(128) k_halfsweep_3d(word_t* __restrict__ s,
                                                       const word_t* __restrict__ J, int L,
                                                       unsigned long long seed,
                                                       unsigned long long draw, int c,
-                                                      Thresholds thr) {
+                                                      Thresholds thr, const uint64_t* __restrict__ draws = nullptr,
+                                                      ThresholdsMT tm = {}) {
   const int hL = L >> 1;
   const long plane = (long)L * hL;  // columns per colour
   const long half = plane * L;
@@ -116,11 +141,20 @@ __global__ void __launch_bounds__(128) k_halfsweep_3d(word_t* __restrict__ s,
     word_t ms = Jy_o[(ys + (long)L * z) * hL + k] ^ so[(ys + (long)L * z) * hL + k] ^ si;
     word_t mu = Jz_c[idx] ^ prev ^ si;
     word_t md = Jz_c[rd * hL + k] ^ sd ^ si;
-    const unsigned long long site = (unsigned long long)x + (unsigned long long)L * r;
-    uint32_t u = philox_draw(seed, site, draw);
     word_t c0, c1, c2;
     count6(mw, me, mn, ms, mu, md, c0, c1, c2);
-    word_t ns = flip_word(si, c0, c1, c2, prefix_count<6>(u, thr.dn), prefix_count<6>(u, thr.up));
+    uint32_t tdn, tup;
+    if (MT) {
+      const uint64_t g = draws[idx];
+      tdn = prefix_count_mt<6>(g, tm.dn, tm.ndn);
+      tup = prefix_count_mt<6>(g, tm.up, tm.nup);
+    } else {
+      const unsigned long long site = (unsigned long long)x + (unsigned long long)L * r;
+      const uint32_t u = philox_draw(seed, site, draw);
+      tdn = prefix_count<6>(u, thr.dn);
+      tup = prefix_count<6>(u, thr.up);
+    }
+    word_t ns = flip_word(si, c0, c1, c2, tdn, tup);
     sc[idx] = ns;
     if (z == 0) first = ns;
     prev = ns;
@@ -204,6 +238,70 @@ __global__ void k_init_rand(word_t* __restrict__ s, int L, long N, unsigned long
   s[split_index(i, L, N / 2, L >> 1)] = (word_t)b.x | ((word_t)b.y << 32);
 }
 
+// ---------------------------------------------------------------------------
+// mt19937_64 on the device: one block advances the system's generator state
+// (st[0..311] words, st[312] the index of the next output) by `count` outputs
+// into out[0..count). The twist is the standard recurrence in its three
+// dependency phases (words 0..155 read old words 156..311; words 156..310 read
+// the new words 0..154; word 311 reads the new words 0 and 155), then every
+// output is tempered.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mt64_twist_word(uint64_t a, uint64_t b, uint64_t m) {
+  const uint64_t y = (a & 0xFFFFFFFF80000000ULL) | (b & 0x7FFFFFFFULL);
+  return m ^ (y >> 1) ^ ((y & 1ULL) ? 0xB5026F5AA96619E9ULL : 0ULL);
+}
+
+__device__ __forceinline__ uint64_t mt64_temper(uint64_t z) {
+  z ^= (z >> 29) & 0x5555555555555555ULL;
+  z ^= (z << 17) & 0x71D67FFFEDA60000ULL;
+  z ^= (z << 37) & 0xFFF7EEE000000000ULL;
+  z ^= z >> 43;
+  return z;
+}
+
+__global__ void __launch_bounds__(320) k_mt_gen(uint64_t* __restrict__ st, uint64_t* __restrict__ out, long count) {
+  __shared__ uint64_t mt[kMtN];
+  const int t = threadIdx.x;
+  for (int i = t; i < kMtN; i += blockDim.x) mt[i] = st[i];
+  int idx = (int)st[kMtN];
+  __syncthreads();
+  long pos = 0;
+  while (pos < count) {
+    if (idx >= kMtN) {
+      uint64_t v = 0;
+      if (t < 156) v = mt64_twist_word(mt[t], mt[t + 1], mt[t + 156]);
+      __syncthreads();
+      if (t < 156) mt[t] = v;
+      __syncthreads();
+      if (t >= 156 && t < kMtN - 1) v = mt64_twist_word(mt[t], mt[t + 1], mt[t - 156]);
+      __syncthreads();
+      if (t >= 156 && t < kMtN - 1) mt[t] = v;
+      __syncthreads();
+      if (t == 0) mt[kMtN - 1] = mt64_twist_word(mt[kMtN - 1], mt[0], mt[155]);
+      __syncthreads();
+      idx = 0;
+    }
+    const long n = min((long)(kMtN - idx), count - pos);
+    for (int i = t; i < n; i += blockDim.x) out[pos + i] = mt64_temper(mt[idx + i]);
+    pos += n;
+    idx += (int)n;
+    __syncthreads();  // the next twist rewrites mt
+  }
+  for (int i = t; i < kMtN; i += blockDim.x) st[i] = mt[i];
+  if (t == 0) st[kMtN] = (uint64_t)idx;
+}
+
+// init_J from mt19937_64 outputs: buffer[dim*i + a] is site i's own bond word
+// on axis a (src/cpu_2dp.cpp:243-260, src/cpu_3d.cpp:281-301).
+__global__ void k_init_J_mt(word_t* __restrict__ J, const uint64_t* __restrict__ buf, int L, int dim, long N) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const long half = N / 2;
+  const long dst = split_index(i, L, half, L >> 1);
+  const long c = dst / half, rem = dst - c * half;
+  for (int a = 0; a < dim; ++a) J[(long)(a * 2 + c) * half + rem] = buf[(long)dim * i + a];
+}
+
 __global__ void k_fill(word_t* __restrict__ s, long n, word_t v) {
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) s[i] = v;
@@ -230,7 +328,7 @@ static inline unsigned grid_for(long n, int threads) { return (unsigned)((n + th
 int launch_halfsweep(sa_system* sy, int c, unsigned long long draw) {
   if (sy->lattice == SA_LATTICE_3D) {
     long plane = (long)sy->L * (sy->L / 2);
-    k_halfsweep_3d<<<grid_for(plane, 128), 128, 0, sy->stream>>>(sy->d_s, sy->d_J, sy->L, sy->seed,
+    k_halfsweep_3d<false><<<grid_for(plane, 128), 128, 0, sy->stream>>>(sy->d_s, sy->d_J, sy->L, sy->seed,
                                                                   draw, c, sy->thr);
   } else if (sy->lattice == SA_LATTICE_2D_OPEN_X) {
     k_halfsweep_2d<true><<<grid_for(sy->half, 256), 256, 0, sy->stream>>>(sy->d_s, sy->d_J, sy->L,
@@ -239,6 +337,36 @@ int launch_halfsweep(sa_system* sy, int c, unsigned long long draw) {
     k_halfsweep_2d<false><<<grid_for(sy->half, 256), 256, 0, sy->stream>>>(sy->d_s, sy->d_J, sy->L,
                                                                            sy->seed, draw, c, sy->thr);
   }
+  return SA_OK;
+}
+
+int mt_generate(sa_system* sy, long n) {
+  k_mt_gen<<<1, 320, 0, sy->stream>>>(sy->d_mt, sy->d_draws, n);
+  SA_CUDA_TRY(cudaGetLastError());
+  return SA_OK;
+}
+
+// One sweep in MT mode: the reference visits colour 0 then colour 1, each in
+// row-major order, one draw per site (src/cpu_2dp.cpp:106-114,
+// src/cpu_3d.cpp:94-105); rank row*L/2 + k of colour c is draw c*N/2 + rank.
+int mt_sweep(sa_system* sy) {
+  int st = mt_generate(sy, sy->N);
+  if (st) return st;
+  for (int c = 0; c < 2; ++c) {
+    const uint64_t* dr = sy->d_draws + (long)c * sy->half;
+    if (sy->lattice == SA_LATTICE_3D) {
+      long plane = (long)sy->L * (sy->L / 2);
+      k_halfsweep_3d<true><<<grid_for(plane, 128), 128, 0, sy->stream>>>(sy->d_s, sy->d_J, sy->L, sy->seed, 0, c,
+                                                                        sy->thr, dr, sy->thr_mt);
+    } else if (sy->lattice == SA_LATTICE_2D_OPEN_X) {
+      k_halfsweep_2d<true, true><<<grid_for(sy->half, 256), 256, 0, sy->stream>>>(
+          sy->d_s, sy->d_J, sy->L, sy->seed, 0, c, sy->thr, dr, sy->thr_mt);
+    } else {
+      k_halfsweep_2d<false, true><<<grid_for(sy->half, 256), 256, 0, sy->stream>>>(
+          sy->d_s, sy->d_J, sy->L, sy->seed, 0, c, sy->thr, dr, sy->thr_mt);
+    }
+  }
+  SA_CUDA_TRY(cudaGetLastError());
   return SA_OK;
 }
 
@@ -327,6 +455,7 @@ int sa_sys_create(int lattice, int L, double T, double h, sa_system_t* out) {
   chk(cudaMalloc(&sy->d_stage, sy->N * sizeof(word_t)), "cudaMalloc stage");
   chk(cudaMalloc(&sy->d_counts, 128 * sizeof(unsigned long long)), "cudaMalloc counts");
   chk(cudaMalloc(&sy->d_EM, 128 * sizeof(int64_t)), "cudaMalloc E/M");
+  chk(cudaMalloc(&sy->d_mt, (kMtN + 1) * sizeof(uint64_t)), "cudaMalloc mt state");
   if (st == SA_OK) {
     chk(cudaMemsetAsync(sy->d_s, 0, sy->N * sizeof(word_t), sy->stream), "memset");
     chk(cudaMemsetAsync(sy->d_J, 0, (size_t)sy->dim * sy->N * sizeof(word_t), sy->stream), "memset");
@@ -351,6 +480,8 @@ int sa_sys_destroy(sa_system_t sy) {
   cudaFree(sy->d_stage);
   cudaFree(sy->d_counts);
   cudaFree(sy->d_EM);
+  cudaFree(sy->d_mt);
+  cudaFree(sy->d_draws);
   if (sy->own_stream) cudaStreamDestroy(sy->own_stream);
   delete sy;
   return SA_OK;
@@ -367,8 +498,12 @@ int sa_sys_set_T(sa_system_t sy, double T) {
   if (!(T > 0)) return fail(SA_ERR_INVALID, "T must be > 0");
   Thresholds t;
   if (!make_thresholds(sy->lattice, T, sy->h, &t)) return fail(SA_ERR_INVALID, "non-monotone table");
+  ThresholdsMT tm;
+  if (sy->rng_mode == SA_RNG_MT19937_64 && !make_thresholds_mt(sy->lattice, T, sy->h, &tm))
+    return fail(SA_ERR_INVALID, "non-monotone table");
   sy->T = T;
   sy->thr = t;  // kernel argument: later launches see it, earlier ones keep theirs
+  if (sy->rng_mode == SA_RNG_MT19937_64) sy->thr_mt = tm;
   return SA_OK;
 }
 
@@ -376,8 +511,12 @@ int sa_sys_set_h(sa_system_t sy, double h) {
   if (!sy) return fail(SA_ERR_INVALID, "null system");
   Thresholds t;
   if (!make_thresholds(sy->lattice, sy->T, h, &t)) return fail(SA_ERR_INVALID, "non-monotone table");
+  ThresholdsMT tm;
+  if (sy->rng_mode == SA_RNG_MT19937_64 && !make_thresholds_mt(sy->lattice, sy->T, h, &tm))
+    return fail(SA_ERR_INVALID, "non-monotone table");
   sy->h = h;
   sy->thr = t;
+  if (sy->rng_mode == SA_RNG_MT19937_64) sy->thr_mt = tm;
   return SA_OK;
 }
 
@@ -387,16 +526,55 @@ int sa_sys_get_T(sa_system_t sy, double* T) {
   return SA_OK;
 }
 
+// MT mode: the device generator restarts from `seed` (gen.seed(seed),
+// src/cpu_3d.cpp:210). The state is built on the host (312 words).
+static int mt_reseed(sa_system* sy) {
+  uint64_t st[kMtN + 1];
+  mt64_seed(sy->seed, st);
+  SA_CUDA_TRY(cudaMemcpyAsync(sy->d_mt, st, sizeof st, cudaMemcpyHostToDevice, sy->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(sy->stream));  // st is on this stack frame
+  return SA_OK;
+}
+
 int sa_sys_set_seed(sa_system_t sy, uint64_t seed) {
   if (!sy) return fail(SA_ERR_INVALID, "null system");
   sy->seed = seed;
   sy->draw = 0;
   sy->epoch = 0;
+  if (sy->rng_mode == SA_RNG_MT19937_64) return mt_reseed(sy);
+  return SA_OK;
+}
+
+int sa_sys_set_rng_mode(sa_system_t sy, int mode) {
+  if (!sy) return fail(SA_ERR_INVALID, "null system");
+  if (mode != SA_RNG_PHILOX && mode != SA_RNG_MT19937_64) return fail(SA_ERR_INVALID, "unknown random mode");
+  if (mode == SA_RNG_MT19937_64) {
+    ThresholdsMT tm;
+    if (!make_thresholds_mt(sy->lattice, sy->T, sy->h, &tm)) return fail(SA_ERR_INVALID, "non-monotone table");
+    if (!sy->d_draws) SA_CUDA_TRY(cudaMalloc(&sy->d_draws, (size_t)sy->dim * sy->N * sizeof(uint64_t)));
+    sy->thr_mt = tm;
+    sy->rng_mode = mode;
+    return mt_reseed(sy);
+  }
+  sy->rng_mode = mode;
+  return SA_OK;
+}
+
+int sa_sys_get_rng_mode(sa_system_t sy, int* mode) {
+  if (!sy || !mode) return fail(SA_ERR_INVALID, "null argument");
+  *mode = sy->rng_mode;
   return SA_OK;
 }
 
 int sa_sys_init_J(sa_system_t sy) {
   if (!sy) return fail(SA_ERR_INVALID, "null system");
+  if (sy->rng_mode == SA_RNG_MT19937_64) {
+    int st = mt_generate(sy, (long)sy->dim * sy->N);
+    if (st) return st;
+    k_init_J_mt<<<grid_for(sy->N, 256), 256, 0, sy->stream>>>(sy->d_J, sy->d_draws, sy->L, sy->dim, sy->N);
+    SA_CUDA_TRY(cudaGetLastError());
+    return SA_OK;
+  }
   k_init_J<<<grid_for(sy->N, 256), 256, 0, sy->stream>>>(sy->d_J, sy->L, sy->dim, sy->N, sy->seed,
                                                           sy->draw);
   SA_CUDA_TRY(cudaGetLastError());
@@ -406,6 +584,15 @@ int sa_sys_init_J(sa_system_t sy) {
 
 int sa_sys_init_rand(sa_system_t sy) {
   if (!sy) return fail(SA_ERR_INVALID, "null system");
+  if (sy->rng_mode == SA_RNG_MT19937_64) {
+    // s[i] = gen() in row-major order (src/cpu_2dp.cpp:222-226, src/cpu_3d.cpp:257-263)
+    int st = mt_generate(sy, sy->N);
+    if (st) return st;
+    k_rowmajor_to_split<<<grid_for(sy->N, 256), 256, 0, sy->stream>>>((const word_t*)sy->d_draws, sy->d_s, sy->L,
+                                                                    sy->N);
+    SA_CUDA_TRY(cudaGetLastError());
+    return SA_OK;
+  }
   k_init_rand<<<grid_for(sy->N, 256), 256, 0, sy->stream>>>(sy->d_s, sy->L, sy->N, sy->seed, sy->epoch);
   SA_CUDA_TRY(cudaGetLastError());
   sy->epoch += 1;
@@ -501,6 +688,13 @@ int sa_sys_get_J(sa_system_t sy, uint64_t* jx, uint64_t* jy, uint64_t* jz) {
 int sa_sys_sweep(sa_system_t sy, long nsweeps) {
   if (!sy) return fail(SA_ERR_INVALID, "null system");
   if (nsweeps < 0) return fail(SA_ERR_INVALID, "nsweeps < 0");
+  if (sy->rng_mode == SA_RNG_MT19937_64) {
+    for (long k = 0; k < nsweeps; ++k) {
+      int st = mt_sweep(sy);
+      if (st) return st;
+    }
+    return SA_OK;
+  }
   if (nsweeps >= kResidentMinSweeps && nsweeps <= 0x7FFFFFFF && resident_ok(sy)) {
     // long runs at zero field: one launch of the resident kernel
     const double T = sy->T;
@@ -603,14 +797,15 @@ struct CkptHeader {
 
 int sa_sys_save(sa_system_t sy, void* buf, size_t cap, size_t* len) {
   if (!sy || !len) return fail(SA_ERR_INVALID, "null argument");
-  size_t need = sizeof(CkptHeader) + (size_t)(1 + sy->dim) * sy->N * sizeof(word_t);
+  const size_t mt_bytes = (sy->rng_mode == SA_RNG_MT19937_64) ? (kMtN + 1) * sizeof(uint64_t) : 0;
+  size_t need = sizeof(CkptHeader) + (size_t)(1 + sy->dim) * sy->N * sizeof(word_t) + mt_bytes;
   *len = need;
   if (!buf) return SA_OK;
   if (cap < need) return fail(SA_ERR_BUFFER, "checkpoint buffer too small");
   CkptHeader hd;
   memset(&hd, 0, sizeof hd);
   memcpy(hd.magic, "SAB200CK", 8);
-  hd.version = 1;
+  hd.version = mt_bytes ? 2 : 1;  // 2: mt19937_64 mode, generator state appended
   hd.lattice = sy->lattice;
   hd.L = sy->L;
   hd.T = sy->T;
@@ -625,6 +820,8 @@ int sa_sys_save(sa_system_t sy, void* buf, size_t cap, size_t* len) {
   p += sy->N * sizeof(word_t);
   SA_CUDA_TRY(cudaMemcpyAsync(p, sy->d_J, (size_t)sy->dim * sy->N * sizeof(word_t),
                               cudaMemcpyDeviceToHost, sy->stream));
+  p += (size_t)sy->dim * sy->N * sizeof(word_t);
+  if (mt_bytes) SA_CUDA_TRY(cudaMemcpyAsync(p, sy->d_mt, mt_bytes, cudaMemcpyDeviceToHost, sy->stream));
   SA_CUDA_TRY(cudaStreamSynchronize(sy->stream));
   return SA_OK;
 }
@@ -634,21 +831,31 @@ int sa_sys_load(sa_system_t sy, const void* buf, size_t len) {
   if (len < sizeof(CkptHeader)) return fail(SA_ERR_BUFFER, "checkpoint truncated");
   CkptHeader hd;
   memcpy(&hd, buf, sizeof hd);
-  if (memcmp(hd.magic, "SAB200CK", 8) != 0 || hd.version != 1)
+  if (memcmp(hd.magic, "SAB200CK", 8) != 0 || (hd.version != 1 && hd.version != 2))
     return fail(SA_ERR_BUFFER, "not a checkpoint of this engine");
   if (hd.lattice != sy->lattice || hd.L != sy->L)
     return fail(SA_ERR_MISMATCH, "checkpoint is for another lattice shape");
-  size_t need = sizeof(CkptHeader) + (size_t)(1 + sy->dim) * sy->N * sizeof(word_t);
+  const bool mt = hd.version == 2;
+  const size_t mt_bytes = mt ? (kMtN + 1) * sizeof(uint64_t) : 0;
+  size_t need = sizeof(CkptHeader) + (size_t)(1 + sy->dim) * sy->N * sizeof(word_t) + mt_bytes;
   if (len < need) return fail(SA_ERR_BUFFER, "checkpoint truncated");
   Thresholds t;
   if (!(hd.T > 0) || !make_thresholds(sy->lattice, hd.T, hd.h, &t))
     return fail(SA_ERR_BUFFER, "checkpoint has a bad temperature");
+  ThresholdsMT tm;
+  if (mt && !make_thresholds_mt(sy->lattice, hd.T, hd.h, &tm))
+    return fail(SA_ERR_BUFFER, "checkpoint has a bad temperature");
+  if (mt && !sy->d_draws) SA_CUDA_TRY(cudaMalloc(&sy->d_draws, (size_t)sy->dim * sy->N * sizeof(uint64_t)));
   const char* p = (const char*)buf + sizeof hd;
   SA_CUDA_TRY(cudaMemcpyAsync(sy->d_s, p, sy->N * sizeof(word_t), cudaMemcpyHostToDevice, sy->stream));
   p += sy->N * sizeof(word_t);
   SA_CUDA_TRY(cudaMemcpyAsync(sy->d_J, p, (size_t)sy->dim * sy->N * sizeof(word_t),
                               cudaMemcpyHostToDevice, sy->stream));
+  p += (size_t)sy->dim * sy->N * sizeof(word_t);
+  if (mt) SA_CUDA_TRY(cudaMemcpyAsync(sy->d_mt, p, mt_bytes, cudaMemcpyHostToDevice, sy->stream));
   SA_CUDA_TRY(cudaStreamSynchronize(sy->stream));
+  sy->rng_mode = mt ? SA_RNG_MT19937_64 : SA_RNG_PHILOX;
+  if (mt) sy->thr_mt = tm;
   sy->T = hd.T;
   sy->h = hd.h;
   sy->thr = t;

@@ -17,10 +17,21 @@ struct sa_system {
   unsigned long long* d_counts = nullptr;  // measure scratch (128 counters)
   int64_t* d_EM = nullptr;         // measure output E[64], M[64]
   sa::Thresholds thr{};
+  // Random-number mode: SA_RNG_PHILOX (the GPU reference's schedule; seed and
+  // draw counter above) or SA_RNG_MT19937_64 (the CPU reference's stream; its
+  // state lives on the device in d_mt, the pass's outputs in d_draws).
+  int rng_mode = 0;
+  uint64_t* d_mt = nullptr;        // [kMtN + 1]: state words, next index
+  uint64_t* d_draws = nullptr;     // dim * N outputs (init_J is the largest pass)
+  sa::ThresholdsMT thr_mt{};
 };
 
 namespace sa {
 int launch_halfsweep(sa_system* sy, int c, unsigned long long draw);
+// MT mode: one sweep drawing its N outputs from the device generator.
+int mt_sweep(sa_system* sy);
+// MT mode: the device generator's next n outputs into d_draws.
+int mt_generate(sa_system* sy, long n);
 int launch_measure(sa_system* sy, int64_t* d_E, int64_t* d_M);
 // The shared-memory-resident batch kernel applied to one system (zero field,
 // L >= 4): nsteps steps of `sweeps` sweeps at T[k], -H measured every `stride`

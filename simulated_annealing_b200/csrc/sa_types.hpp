@@ -19,5 +19,23 @@ struct Thresholds {
   uint32_t bup[8];  // open-x border sites, spin up:   boltz[15..19]
 };
 
+// The same tables for the CPU reference's generator: a 64-bit mt19937_64
+// output g becomes the double u(g) = min(fl(g) * 2^-64, 1 - 2^-53) (libstdc++
+// generate_canonical<double, 53> + uniform_real_distribution(0, 1)), compared
+// as double with the double table. u is non-decreasing in g, so "accept" is
+// g <= thr[k] with thr[k] the largest accepted g. Entries whose Boltzmann
+// factor underflows to 0 accept nothing; they are the last ones of a table
+// (the factor falls with k), so each table keeps the number n* of entries
+// that accept anything and the prefix counts only those.
+struct ThresholdsMT {
+  uint64_t dn[8], up[8], bdn[8], bup[8];
+  int ndn, nup, nbdn, nbup;
+};
+
+// mt19937_64 (Matsumoto & Nishimura, the C++ standard's predefined engine):
+// 312 state words; the state block on the device holds the words and then
+// the index of the next output.
+constexpr int kMtN = 312;
+
 
 }  // namespace sa

@@ -58,6 +58,19 @@ class GpuSystem:
     def set_seed(self, seed: int) -> None:
         check(self._lib.sa_sys_set_seed(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF))
 
+    def set_rng_mode(self, mode) -> None:
+        """'philox' (default: the GPU reference's cuRAND schedule) or 'mt19937_64'
+        (the CPU reference's stream, bit-exact with cpu_2d/cpu_2dp/cpu_3d).
+        Switching reseeds the generator with the current seed."""
+        if isinstance(mode, str):
+            mode = {"philox": _lib.SA_RNG_PHILOX, "mt19937_64": _lib.SA_RNG_MT19937_64}[mode]
+        check(self._lib.sa_sys_set_rng_mode(self._h, int(mode)))
+
+    def rng_mode(self) -> int:
+        m = ctypes.c_int()
+        check(self._lib.sa_sys_get_rng_mode(self._h, ctypes.byref(m)))
+        return m.value
+
     def measure(self) -> list[float]:
         out = np.zeros(64, dtype=np.float32)
         check(self._lib.sa_sys_measure_float(self._h, _p(out, ctypes.c_float)))
