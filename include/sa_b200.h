@@ -128,6 +128,15 @@ int sa_sys_get_N(sa_system_t sys, long* N);
  *   Switching to it reseeds the generator with the current seed. */
 int sa_sys_set_rng_mode(sa_system_t sys, int mode);
 int sa_sys_get_rng_mode(sa_system_t sys, int* mode);
+/* The reference CPU classes' own checkpoint record, byte for byte as
+ * cpu_2dp::save / cpu_3d::save write it (src/cpu_2dp.cpp:444-456,
+ * src/cpu_3d.cpp:449-461): L, T, h, spins, the reference-layout couplings and
+ * the std::mt19937_64 state. Saving needs SA_RNG_MT19937_64 mode (the record
+ * carries that generator); loading switches the system to it, so a run can
+ * move between the reference's CPU binary and this engine mid-stream.
+ * buf == NULL: *len receives the size. */
+int sa_sys_save_reference(sa_system_t sys, void* buf, size_t cap, size_t* len);
+int sa_sys_load_reference(sa_system_t sys, const void* buf, size_t len);
 /* RNG position (for checkpoints): draw counter and spin-init epoch. */
 int sa_sys_get_rng(sa_system_t sys, uint64_t* seed, uint64_t* draw, uint64_t* epoch);
 int sa_sys_set_rng(sa_system_t sys, uint64_t seed, uint64_t draw, uint64_t epoch);

@@ -135,6 +135,9 @@ def ref_lib():
         lib.ref_pt_free.argtypes = [_vp]
         lib.ref_anneal_run.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, _f32p]
+        lib.ref_save.restype = ctypes.c_long
+        lib.ref_save.argtypes = [_vp, ctypes.c_char_p, ctypes.c_long]
+        lib.ref_load.argtypes = [_vp, ctypes.c_char_p, ctypes.c_long]
         _REF = lib
     return _REF
 
@@ -336,6 +339,15 @@ class RefSystem:
 
     def swap(self, other, mask):
         self.lib.ref_swap(self.h, other.h, mask)
+
+    def save(self) -> bytes:
+        n = self.lib.ref_save(self.h, None, 0)
+        buf = ctypes.create_string_buffer(n)
+        self.lib.ref_save(self.h, buf, n)
+        return buf.raw[:n]
+
+    def load(self, data: bytes) -> None:
+        self.lib.ref_load(self.h, data, len(data))
 
     def anneal(self, T0, alfa, nsteps, sweeps, stride=1):
         mn = np.zeros(64, dtype=np.float32)

@@ -182,4 +182,20 @@ void ref_anneal_run(void* p, double T0, double alfa, int nsteps, int sweeps, int
   for (int j = 0; j < 64; ++j) in >> min_E[j];
 }
 
+// The reference object's own save() / load() byte stream (its checkpoint
+// record), for comparing this engine's record with it.
+long ref_save(void* p, char* buf, long cap) {
+  RefSys* r = (RefSys*)p;
+  std::stringstream ss;
+  r->sys->save(ss);
+  std::string b = ss.str();
+  if (buf && cap >= (long)b.size()) memcpy(buf, b.data(), b.size());
+  return (long)b.size();
+}
+void ref_load(void* p, const char* buf, long len) {
+  RefSys* r = (RefSys*)p;
+  std::stringstream ss(std::string(buf, (size_t)len));
+  r->sys->load(ss);
+}
+
 }  // extern "C"

@@ -75,6 +75,8 @@ _PROTOS = {
     "sa_sys_get_rng": (_c.c_int, [_vp, _u64p, _u64p, _u64p]),
     "sa_sys_set_rng_mode": (_c.c_int, [_vp, _c.c_int]),
     "sa_sys_get_rng_mode": (_c.c_int, [_vp, _c.POINTER(_c.c_int)]),
+    "sa_sys_save_reference": (_c.c_int, [_vp, _vp, _c.c_size_t, _szp]),
+    "sa_sys_load_reference": (_c.c_int, [_vp, _vp, _c.c_size_t]),
     "sa_sys_set_rng": (_c.c_int, [_vp, _u64, _u64, _u64]),
     "sa_sys_sync": (_c.c_int, [_vp]),
     "sa_sys_save": (_c.c_int, [_vp, _vp, _c.c_size_t, _szp]),

@@ -865,4 +865,85 @@ int sa_sys_load(sa_system_t sy, const void* buf, size_t len) {
   return SA_OK;
 }
 
+// ---- the reference CPU classes' checkpoint record (mt19937_64 mode) --------
+// cpu_2dp::save / cpu_3d::save (src/cpu_2dp.cpp:444-456, src/cpu_3d.cpp:449-461)
+// write, in this order: int L; double T; double h; s[N]; Jx[2N]; Jy[2N];
+// (Jz[2N]); the std::mt19937_64 object (312 state words, then the size_t index
+// of the next output -- libstdc++'s layout); uniform_real_distribution<double>
+// (a, b); uniform_int_distribution<int> (a, b). Only the generator part has
+// meaning here; the distributions are written as the reference sets them up.
+static size_t ref_record_size(const sa_system* sy) {
+  return sizeof(int32_t) + 2 * sizeof(double) + (size_t)sy->N * 8 + (size_t)sy->dim * 2 * sy->N * 8 +
+         (kMtN + 1) * sizeof(uint64_t) + 2 * sizeof(double) + 2 * sizeof(int32_t);
+}
+
+int sa_sys_save_reference(sa_system_t sy, void* buf, size_t cap, size_t* len) {
+  if (!sy || !len) return fail(SA_ERR_INVALID, "null argument");
+  if (sy->rng_mode != SA_RNG_MT19937_64)
+    return fail(SA_ERR_UNSUPPORTED, "the reference record holds an mt19937_64 generator: set that mode first");
+  const size_t need = ref_record_size(sy);
+  *len = need;
+  if (!buf) return SA_OK;
+  if (cap < need) return fail(SA_ERR_BUFFER, "buffer too small");
+  std::vector<uint64_t> sp(sy->N), J[3];
+  for (int a = 0; a < sy->dim; ++a) J[a].resize(2 * sy->N);
+  int st = sa_sys_get_spins(sy, sp.data());
+  if (st == SA_OK) st = sa_sys_get_J(sy, J[0].data(), J[1].data(), sy->dim == 3 ? J[2].data() : nullptr);
+  if (st != SA_OK) return st;
+  uint64_t mt[kMtN + 1];
+  SA_CUDA_TRY(cudaMemcpyAsync(mt, sy->d_mt, sizeof mt, cudaMemcpyDeviceToHost, sy->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(sy->stream));
+  char* p = (char*)buf;
+  auto put = [&](const void* src, size_t n) {
+    memcpy(p, src, n);
+    p += n;
+  };
+  const int32_t L = sy->L;
+  put(&L, sizeof L);
+  put(&sy->T, sizeof(double));
+  put(&sy->h, sizeof(double));
+  put(sp.data(), sp.size() * 8);
+  for (int a = 0; a < sy->dim; ++a) put(J[a].data(), J[a].size() * 8);
+  put(mt, sizeof mt);
+  const double ud[2] = {0.0, 1.0};
+  const int32_t ui[2] = {0, (int32_t)(sy->N - 1)};
+  put(ud, sizeof ud);
+  put(ui, sizeof ui);
+  return SA_OK;
+}
+
+int sa_sys_load_reference(sa_system_t sy, const void* buf, size_t len) {
+  if (!sy || !buf) return fail(SA_ERR_INVALID, "null argument");
+  if (len < ref_record_size(sy)) return fail(SA_ERR_BUFFER, "record truncated or for another lattice size");
+  const char* p = (const char*)buf;
+  auto get = [&](void* dst, size_t n) {
+    memcpy(dst, p, n);
+    p += n;
+  };
+  int32_t L;
+  double T, h;
+  get(&L, sizeof L);
+  get(&T, sizeof T);
+  get(&h, sizeof h);
+  if (L != sy->L) return fail(SA_ERR_MISMATCH, "record is for another lattice size");
+  std::vector<uint64_t> sp(sy->N), J[3];
+  get(sp.data(), sp.size() * 8);
+  for (int a = 0; a < sy->dim; ++a) {
+    J[a].resize(2 * sy->N);
+    get(J[a].data(), J[a].size() * 8);
+  }
+  uint64_t mt[kMtN + 1];
+  get(mt, sizeof mt);
+  if (mt[kMtN] > (uint64_t)kMtN) return fail(SA_ERR_BUFFER, "bad generator index in the record");
+  int st = sa_sys_set_rng_mode(sy, SA_RNG_MT19937_64);
+  if (st == SA_OK) st = sa_sys_set_h(sy, h);
+  if (st == SA_OK) st = sa_sys_set_T(sy, T);
+  if (st == SA_OK) st = sa_sys_set_J(sy, J[0].data(), J[1].data(), sy->dim == 3 ? J[2].data() : nullptr);
+  if (st == SA_OK) st = sa_sys_set_spins(sy, sp.data());
+  if (st != SA_OK) return st;
+  SA_CUDA_TRY(cudaMemcpyAsync(sy->d_mt, mt, sizeof mt, cudaMemcpyHostToDevice, sy->stream));
+  SA_CUDA_TRY(cudaStreamSynchronize(sy->stream));
+  return SA_OK;
+}
+
 }  // extern "C"

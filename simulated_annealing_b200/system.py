@@ -143,6 +143,19 @@ class GpuSystem:
         buf = ctypes.create_string_buffer(data, len(data))
         check(self._lib.sa_sys_load(self._h, buf, len(data)))
 
+    def save_reference(self) -> bytes:
+        """The record cpu_2dp::save / cpu_3d::save write (mt19937_64 mode)."""
+        n = ctypes.c_size_t()
+        check(self._lib.sa_sys_save_reference(self._h, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        check(self._lib.sa_sys_save_reference(self._h, buf, n.value, ctypes.byref(n)))
+        return buf.raw[: n.value]
+
+    def load_reference(self, data: bytes) -> None:
+        """Load a cpu_2dp / cpu_3d record; switches to mt19937_64 mode."""
+        buf = ctypes.create_string_buffer(data, len(data))
+        check(self._lib.sa_sys_load_reference(self._h, buf, len(data)))
+
     def anneal(self, T, sweeps: int, stride: int = 1):
         """annealing<gpu_sys> on the device over the schedule T (one entry per
         step of `sweeps` sweeps). Returns (min_E float[64], step_E int64[nsteps, 64])."""

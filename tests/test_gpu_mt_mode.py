@@ -128,3 +128,31 @@ def test_switching_back_to_philox_follows_the_oracle(sab):
         x.init_rand()
         x.sweep(5)
     assert np.array_equal(g.get_spins(), o.spins())
+
+
+@pytest.mark.parametrize("lat,L", [(O.LAT_2D, 6), (O.LAT_2D_OPEN_X, 8), (O.LAT_3D, 4)])
+def test_reference_checkpoint_record_both_ways(sab, lat, L):
+    """The engine writes the reference classes' save() record byte for byte,
+    and a record the reference wrote continues here draw for draw."""
+    g, r = _mt(lat, L, 1.3, 0.2), O.RefSystem(lat, L, 1.3, 0.2)
+    for x in (g, r):
+        x.set_seed(21)
+        x.init_J()
+        x.set_seed(22)
+        x.init_rand()
+        x.sweep(3)
+    assert g.save_reference() == r.save()
+    # reference -> engine: a fresh system picks up the stream mid-way
+    from simulated_annealing_b200.system import GpuSystem
+    h = GpuSystem(lat, L, 2.0)
+    h.load_reference(r.save())
+    assert h.rng_mode() == 1
+    h.sweep(5)
+    r.sweep(5)
+    _same(h, r)
+    # engine -> reference
+    r2 = O.RefSystem(lat, L)
+    r2.load(h.save_reference())
+    h.sweep(4)
+    r2.sweep(4)
+    _same(h, r2)
