@@ -186,38 +186,68 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
   const word_t* Jyc = x.J + (long)(2 + c) * x.half;
   const word_t* Jyo = x.J + (long)(3 - c) * x.half;
   for (int base = warp * 32; base < tot; base += nwarps * 32) {
+    // Lane i of the warp prepares site base+i once: its Philox draw, its four
+    // coupling words, its row offsets, its neighbours' swizzles and its border
+    // flags. The P lanes updating that site's slots fetch them by shuffles
+    // instead of each recomputing the indices and reloading the couplings.
     const int my = base + lane;
-    uint32_t um = 0;
+    uint32_t um = 0, pk = 0, nadr = 0, sadr = 0;
+    int rowc = 0, roww = 0, rowe = 0;
+    word_t bw = 0, be = 0, bn = 0, bs = 0;
     if (my < tot) {
       const int yl = div_hl(my, x);
       const int k = my - yl * hL, y = x.y0 + yl;
-      const int xx = 2 * k + ((c + y) & 1);
+      const int par = (c + y) & 1, xx = 2 * k + par;
+      int kw, ke;
+      x_neighbours(k, par, hL, kw, ke);
+      const int ys = (y == L - 1) ? 0 : y + 1;
       um = philox_draw(x.seed, (unsigned long long)(xx + L * y), draw);
+      bw = __ldg(Jxc + y * hL + k);
+      be = __ldg(Jxo + y * hL + ke);
+      bn = __ldg(Jyc + y * hL + k);
+      bs = __ldg(Jyo + ys * hL + k);
+      rowc = lrow(x, c, 0, yl) + k * ns;
+      roww = lrow(x, oc, 0, yl) + kw * ns;
+      rowe = lrow(x, oc, 0, yl) + ke * ns;
+      // swizzles (< 32) of k, kw, ke and the border flags in one word
+      pk = (uint32_t)swz(x, k) | ((uint32_t)swz(x, kw) << 8) | ((uint32_t)swz(x, ke) << 16) |
+           ((OPEN_X && xx == 0) ? (1u << 24) : 0u) | ((OPEN_X && xx == L - 1) ? (1u << 25) : 0u);
+      const NbRow<CL> pn = north_row<CL>(x, oc, 0, yl), ps = south_row<CL>(x, oc, 0, yl);
+      if constexpr (CL) {
+        nadr = pn.a + 8u * (uint32_t)(k * ns);
+        sadr = ps.a + 8u * (uint32_t)(k * ns);
+      } else {
+        nadr = (uint32_t)(pn.p - x.sm) + (uint32_t)(k * ns);  // word offsets in this CTA
+        sadr = (uint32_t)(ps.p - x.sm) + (uint32_t)(k * ns);
+      }
     }
 #pragma unroll 1
     for (int sub = 0; sub < P; ++sub) {
       const int sl = sub * SPS + lane / P;
-      const uint32_t u = __shfl_sync(0xffffffffu, um, sl);
+      // one lane per site (P = 1): the lane's own values
+      auto share = [&](auto v) { return (P == 1) ? v : __shfl_sync(0xffffffffu, v, sl); };
+      const uint32_t u = share(um);
+      const word_t jw = share(bw), je = share(be), jn = share(bn), js = share(bs);
+      const int rc = share(rowc), rw = share(roww), re = share(rowe);
+      const uint32_t f = share(pk), na = share(nadr), sa = share(sadr);
       const int t = base + sl;
       if (t < tot && slot_ok) {
-        const int yl = div_hl(t, x);
-        const int k = t - yl * hL, y = x.y0 + yl;
-        const int par = (c + y) & 1, xx = 2 * k + par;
-        int kw, ke;
-        x_neighbours(k, par, hL, kw, ke);
-        const int sk = slot ^ swz(x, k);
-        const int own = lrow(x, c, 0, yl) + k * ns + sk;
-        const int orow = lrow(x, oc, 0, yl);
-        const NbRow<CL> pn = north_row<CL>(x, oc, 0, yl), ps = south_row<CL>(x, oc, 0, yl);
-        const int ys = (y == L - 1) ? 0 : y + 1;
+        const int sk = slot ^ (int)(f & 0xFFu);
+        const int own = rc + sk;
         const SlotWords<SL> si = ldw<SL>(x.sm + own);
-        const SlotWords<SL> sw = ldw<SL>(x.sm + orow + kw * ns + (slot ^ swz(x, kw)));
-        const SlotWords<SL> se = ldw<SL>(x.sm + orow + ke * ns + (slot ^ swz(x, ke)));
-        const SlotWords<SL> sn = pn.template ld<SL>(k * ns + sk);
-        const SlotWords<SL> ss = ps.template ld<SL>(k * ns + sk);
-        const word_t jw = __ldg(Jxc + y * hL + k), je = __ldg(Jxo + y * hL + ke);
-        const word_t jn = __ldg(Jyc + y * hL + k), js = __ldg(Jyo + ys * hL + k);
-        const bool border = OPEN_X && (xx == 0 || xx == L - 1);
+        const SlotWords<SL> sw = ldw<SL>(x.sm + rw + (slot ^ (int)((f >> 8) & 0xFFu)));
+        const SlotWords<SL> se = ldw<SL>(x.sm + re + (slot ^ (int)((f >> 16) & 0xFFu)));
+        SlotWords<SL> sn, ss;
+        if constexpr (CL) {
+          sn = ldc<SL>(na + 8u * (uint32_t)sk);
+          ss = ldc<SL>(sa + 8u * (uint32_t)sk);
+        } else {
+          sn = ldw<SL>(x.sm + na + sk);
+          ss = ldw<SL>(x.sm + sa + sk);
+        }
+        const bool bwest = OPEN_X && (f & (1u << 24));
+        const bool beast = OPEN_X && (f & (1u << 25));
+        const bool border = bwest || beast;
         SlotWords<SL> out;
 #pragma unroll
         for (int q = 0; q < SL; ++q) {
@@ -226,8 +256,8 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
           const word_t mn = jn ^ sn.w[q] ^ si.w[q];
           const word_t ms = js ^ ss.w[q] ^ si.w[q];
           if (OPEN_X) {
-            if (xx == 0) mw = ~0ULL;
-            if (xx == L - 1) me = ~0ULL;
+            if (bwest) mw = ~0ULL;
+            if (beast) me = ~0ULL;
           }
           word_t c0, c1, c2;
           count4(mw, me, mn, ms, c0, c1, c2);
