@@ -363,8 +363,10 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchParams p) {
 // LAT: lattice kind of every instance of the launch; CL: clusters of more
 // than one CTA (DSMEM halos and cluster barriers) or single CTAs (block
 // barriers only).
-template <int P, int SL, int LAT, bool CL>
-__global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
+// SEG: single-slot 3D instances spread over many SMs walk their columns in
+// segments (rhalf_3d1s) instead of whole (rhalf_3d1).
+template <int P, int SL, int LAT, bool CL, bool SEG = false>
+__global__ void __launch_bounds__(SEG ? kSegMaxThreads : kResMaxThreads, 1) k_resident(BatchParams p) {
   extern __shared__ __align__(16) word_t s_spins[];
   __shared__ unsigned s_cnt[2][64];   // this CTA's partial counts
   __shared__ unsigned s_tot[2][64];   // cluster totals
@@ -482,7 +484,9 @@ __global__ void __launch_bounds__(kResMaxThreads, 1) k_resident(BatchParams p) {
     }
     for (int c = 0; c < 2; ++c) {
       if (d3) {
-        if (P == 1 && SL == 1 && x.L > 4) rhalf_3d1<2, CL>(x, c, draw + c, th[0]);
+        if constexpr (SEG) {
+          rhalf_3d1s<CL>(x, c, draw + c, th[0]);
+        } else if (P == 1 && SL == 1 && x.L > 4) rhalf_3d1<2, CL>(x, c, draw + c, th[0]);
         else rhalf_3d<P, SL, CL>(x, c, draw + c, th);
       }
       else rhalf_2d<P, SL, open, CL>(x, c, draw + c, th, tb);
@@ -741,12 +745,14 @@ struct sa_batch {
     int threads;        // resident: block size matched to the shape's work
     int lattice, L;     // resident groups hold one shape each
     int SL, RP;         // resident: slots per lane and lanes per site
+    bool seg;           // resident: single-slot 3D walked in column segments
     cudaStream_t stream;
     cudaEvent_t done;
   };
   std::vector<Group> groups;
   cudaEvent_t fork = nullptr;
   std::vector<int> cluster_of;  // per instance: C (0 = global-memory kernel)
+  bool spread = false;          // clusters were enlarged to use idle SMs
 };
 
 // Shared-memory budget of one CTA of the resident kernel: the 227 KB opt-in
@@ -825,7 +831,9 @@ static void spread_clusters(sa_batch* b) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
   long total = 0;
   for (int C : b->cluster_of) total += C;
+  b->spread = false;
   if (total == 0 || total * 2 > sms) return;
+  b->spread = true;
   const long factor = sms / total;
   for (size_t i = 0; i < b->inst.size(); ++i) {
     const int C0 = b->cluster_of[i];
@@ -861,8 +869,18 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
     const InstDesc& d = b->inst[order[i]];
     const int C = b->cluster_of[order[i]];
     const size_t smem = C ? resident_bytes(d, C) : 0;
+    // Spread single-slot 3D instances walk columns in segments when a CTA's
+    // columns x lanes fit in at most three passes of the block: there the
+    // chained walk is latency-bound; beyond that it is throughput-bound and the
+    // segments' extra map and scan work costs more than it saves (measured:
+    // 3D L=32 on 16 CTAs 49.8 -> 17.2 us per sweep, L=64 97.6 -> 136.7).
+    bool seg = C != 0 && b->spread && d.lattice == SA_LATTICE_3D && d.nslots == 1 && d.L > 4;
+    if (seg) {
+      const long lanes = (long)((d.L + C - 1) / C) * (d.L / 2) * seg_lanes(d.L);
+      seg = (lanes + kSegMaxThreads - 1) / kSegMaxThreads <= 3;
+    }
     const bool same = !b->groups.empty() && b->groups.back().resident == (C != 0) && b->groups.back().P == d.P &&
-                      b->groups.back().C == C &&
+                      b->groups.back().C == C && b->groups.back().seg == seg &&
                       (C == 0 || (b->groups.back().lattice == d.lattice && b->groups.back().L == d.L));
     if (!same) {
       sa_batch::Group g{};
@@ -875,6 +893,7 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
       g.threads = kBatchThreads;
       g.SL = 1;
       g.RP = d.P;
+      g.seg = seg;
       if (C) {
         // warp passes of one half-sweep: 3D walks columns, 32/RP per pass; 2D
         // takes tiles of 32 sites (RP sub-steps of 32/RP sites each). Two slots
@@ -882,6 +901,11 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
         // slot count is even and there is still work for >= 12 warps.
         const int ny = (d.L + C - 1) / C, hL = d.L / 2;
         auto passes_for = [&](int rp) {
+          if (seg) {
+            // seg_lanes(L) lanes per column
+            const int cpw = 32 / seg_lanes(d.L);
+            return (ny * hL + cpw - 1) / cpw;
+          }
           return (d.lattice == SA_LATTICE_3D) ? (ny * hL + (32 / rp) - 1) / (32 / rp) : (ny * hL + 31) / 32;
         };
         if (d.nslots % 2 == 0) {
@@ -894,7 +918,7 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
           }
         }
         const int passes = passes_for(g.RP);
-        int warps = std::min(passes, kResMaxWarps);
+        int warps = std::min(passes, seg ? kSegMaxThreads / 32 : kResMaxWarps);
         const int rounds = (passes + warps - 1) / warps;
         warps = std::max(4, (passes + rounds - 1) / rounds);
         if (d.nslots == 1 && smem >= 64 * 1024) {
@@ -902,7 +926,7 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
           // every sweep: give the measurement pass (one unit = 32 sites of one
           // colour and plane) at least ~4 units per warp of parallelism
           const int units = 2 * ((d.lattice == SA_LATTICE_3D) ? d.L : 1) * ((ny * hL + 31) / 32);
-          warps = std::max(warps, std::min(kResMaxWarps, (units + 3) / 4));
+          warps = std::max(warps, std::min(seg ? kSegMaxThreads / 32 : kResMaxWarps, (units + 3) / 4));
         }
         g.threads = warps * 32;
       }
@@ -986,6 +1010,8 @@ static int ensure_decisions(sa_batch* b, const std::vector<int64_t>& need) {
 template <int P, int SL>
 static void (*resident_kernel_sl(const sa_batch::Group& g))(BatchParams) {
   const bool cl = g.C > 1;
+  if constexpr (P == 1 && SL == 1)
+    if (g.seg) return cl ? k_resident<1, 1, SA_LATTICE_3D, true, true> : k_resident<1, 1, SA_LATTICE_3D, false, true>;
   if (g.lattice == SA_LATTICE_3D)
     return cl ? k_resident<P, SL, SA_LATTICE_3D, true> : k_resident<P, SL, SA_LATTICE_3D, false>;
   if (g.lattice == SA_LATTICE_2D_OPEN_X)

@@ -26,6 +26,9 @@ namespace cg = cooperative_groups;
 
 constexpr int kResMaxWarps = 20;  // 5 warps per SM sub-partition at <= 96 registers
 constexpr int kResMaxThreads = kResMaxWarps * 32;
+// the segmented single-slot 3D variant trades threads for registers (its
+// segment maps stay in registers): 16 warps at up to 128 registers
+constexpr int kSegMaxThreads = 512;
 
 struct ResCtx {
   word_t* sm;           // this CTA's rows
@@ -493,6 +496,141 @@ __device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw,
           if (z == 0) first = prev;
         }
       }
+    }
+  }
+}
+
+// Lanes per column of the segmented single-slot 3D half-sweep: the smallest
+// power of two that leaves at most kSegMax planes per lane.
+constexpr int kSegMax = 4;
+__host__ __device__ constexpr int seg_lanes(int L) {
+  return L <= kSegMax ? 1 : L <= 2 * kSegMax ? 2 : L <= 4 * kSegMax ? 4 : L <= 8 * kSegMax ? 8 : 16;
+}
+
+// Single-slot 3D half-sweep with every column's z-walk split over G lanes,
+// for instances spread over many SMs (few instances: latency, not throughput,
+// is the limit). Each site's update is an affine map of the new spin below it
+// (see rhalf_3d1): new = A ^ (x & B). Lane g of a column forms the maps of
+// its segment of planes (<= kSegMax, loads and draws independent), composes
+// them into one segment map, and an exclusive scan over the column's G lanes
+// (shuffles) gives every segment its input; the chain into segment 0 is the
+// old top spin. The top plane's z+1 neighbour is the new z = 0 spin, which
+// segment 0 knows after its first map and shares before the other maps are
+// formed. A column's lanes are in one warp and all of them finish reading
+// old values before the scan, so the writes after it cannot race with them.
+template <bool CL>
+__device__ __forceinline__ void rhalf_3d1s(const ResCtx& x, int c, uint64_t draw, const uint32_t* th) {
+  const int G = seg_lanes(x.L);
+  const int CPW = 32 / G;  // columns per warp pass
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane % G, cl = lane / G, lead = cl * G;
+  const int L = x.L, hL = x.hL;
+  const int cols = x.ny * hL;
+  const int oc = 1 - c;
+  const int zs = x.ny * x.rowW;  // local z stride (rowW == hL)
+  const int zg = L * hL;         // z stride of the coupling arrays
+  // segment g: planes [z0, z0 + ls), sizes as even as L allows (ls >= 2)
+  const int sbase = L / G, srem = L % G;
+  const int ls = sbase + (g < srem ? 1 : 0);
+  const int z0 = g * sbase + min(g, srem);
+  const word_t* Jxc = x.J + (long)(0 + c) * x.half;
+  const word_t* Jxo = x.J + (long)(1 - c) * x.half;
+  const word_t* Jyc = x.J + (long)(2 + c) * x.half;
+  const word_t* Jyo = x.J + (long)(3 - c) * x.half;
+  const word_t* Jzc = x.J + (long)(4 + c) * x.half;
+  for (int cb = warp * CPW; cb < cols; cb += nwarps * CPW) {  // warp-uniform
+    const int col = cb + cl;
+    const bool col_ok = col < cols;
+    const int cc = col_ok ? col : 0;
+    const int yl = div_hl(cc, x);
+    const int k = cc - yl * hL;
+    const int y = x.y0 + yl;
+    const int par = (c + y) & 1, xx = 2 * k + par;
+    int kw, ke;
+    x_neighbours(k, par, hL, kw, ke);
+    const int ys = (y == L - 1) ? 0 : y + 1;
+    word_t* own = x.sm + lrow(x, c, 0, yl) + k;
+    const word_t* pw = x.sm + lrow(x, oc, 0, yl) + kw;
+    const word_t* pe = x.sm + lrow(x, oc, 0, yl) + ke;
+    NbRow<CL> pn = north_row<CL>(x, oc, 0, yl), ps = south_row<CL>(x, oc, 0, yl);
+    pn.step(k);
+    ps.step(k);
+    const int zsn = (yl > 0) ? zs : x.nyN * x.rowW;
+    const int zss = (yl < x.ny - 1) ? zs : x.nyS * x.rowW;
+    const int jo = y * hL + k, je = y * hL + ke, js = ys * hL + k;
+    const unsigned long long site0 = (unsigned long long)(xx + L * y), plane = (unsigned long long)L * L;
+    // the old top spin: the chain's input below z = 0
+    const word_t top = __shfl_sync(0xffffffffu, (col_ok && g == 0) ? own[(L - 1) * zs] : 0ULL, lead);
+    word_t A[kSegMax], B[kSegMax];
+    auto site_map = [&](int z, word_t sd, word_t& a, word_t& b) {
+      const int zn = (z == L - 1) ? 0 : z + 1;
+      const word_t si = own[z * zs];
+      const word_t sw = pw[z * zs], se = pe[z * zs];
+      const word_t sn = pn.template ld<1>(z * zsn).w[0], ss = ps.template ld<1>(z * zss).w[0];
+      const word_t jw = __ldg(Jxc + jo + z * zg), jee = __ldg(Jxo + je + z * zg);
+      const word_t jn = __ldg(Jyc + jo + z * zg), jss = __ldg(Jyo + js + z * zg);
+      const word_t ju = __ldg(Jzc + jo + z * zg), jd = __ldg(Jzc + jo + zn * zg);
+      const uint32_t u = philox_draw(x.seed, site0 + plane * (unsigned)z, draw);
+      word_t c0, c1, c2;
+      count5(jw ^ sw ^ si, jee ^ se ^ si, jn ^ sn ^ si, jss ^ ss ^ si, jd ^ sd ^ si, c0, c1, c2);
+      uint32_t m0, m1, m2;
+      prefix_bits(u, th, m0, m1, m2);
+      const uint32_t t = (m0 & 1u) | (m1 & 2u) | (m2 & 4u);
+      const uint32_t t1 = t ? t - 1 : 0;
+      const word_t lo = below(c0, c1, c2, m0, m1, m2);
+      const word_t hi = below(c0, c1, c2, (t1 & 1u) ? ~0u : 0u, (t1 & 2u) ? ~0u : 0u, (t1 & 4u) ? ~0u : 0u);
+      const word_t gg = ju ^ si;
+      const word_t f0 = (gg & hi) | (~gg & lo);
+      a = si ^ f0;
+      b = lo ^ hi;
+    };
+    // first plane of every segment (z0 + 1 < L: segments hold >= 2 planes);
+    // segment 0's gives the new z = 0 spin
+    A[0] = 0;
+    B[0] = 0;
+    if (col_ok) site_map(z0, own[(z0 + 1) * zs], A[0], B[0]);
+    const word_t first = __shfl_sync(0xffffffffu, A[0] ^ (top & B[0]), lead);
+#pragma unroll
+    for (int i = 1; i < kSegMax; ++i) {
+      A[i] = 0;
+      B[i] = 0;
+      if (col_ok && i < ls) {
+        const int z = z0 + i;
+        site_map(z, (z == L - 1) ? first : own[(z + 1) * zs], A[i], B[i]);
+      }
+    }
+    // segment map (first plane applied first), then an inclusive scan over g
+    word_t SA = A[0], SB = B[0];
+#pragma unroll
+    for (int i = 1; i < kSegMax; ++i)
+      if (i < ls) {
+        SA = A[i] ^ (SA & B[i]);
+        SB &= B[i];
+      }
+#pragma unroll 1
+    for (int d = 1; d < G; d <<= 1) {
+      const word_t pA = __shfl_up_sync(0xffffffffu, SA, d, G);
+      const word_t pB = __shfl_up_sync(0xffffffffu, SB, d, G);
+      if (g >= d) {
+        SA = SA ^ (pA & SB);
+        SB = pB & SB;
+      }
+    }
+    // exclusive prefix (identity for g = 0) applied to the old top spin
+    word_t EA = __shfl_up_sync(0xffffffffu, SA, 1, G), EB = __shfl_up_sync(0xffffffffu, SB, 1, G);
+    if (g == 0) {
+      EA = 0;
+      EB = ~0ULL;
+    }
+    __syncwarp();
+    if (col_ok) {
+      word_t v = EA ^ (top & EB);
+#pragma unroll
+      for (int i = 0; i < kSegMax; ++i)
+        if (i < ls) {
+          v = A[i] ^ (v & B[i]);
+          own[(z0 + i) * zs] = v;
+        }
     }
   }
 }
