@@ -363,10 +363,17 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchParams p) {
 // LAT: lattice kind of every instance of the launch; CL: clusters of more
 // than one CTA (DSMEM halos and cluster barriers) or single CTAs (block
 // barriers only).
+// Single-slot 3D variants (segmented walk, fused measurement) hold more state
+// per thread: 16 warps at up to 128 registers.
+template <int P, int SL, int LAT, bool SEG>
+constexpr int res_max_threads() {
+  return (SEG || (P == 1 && SL == 1 && LAT == SA_LATTICE_3D)) ? kSegMaxThreads : kResMaxThreads;
+}
+
 // SEG: single-slot 3D instances spread over many SMs walk their columns in
 // segments (rhalf_3d1s) instead of whole (rhalf_3d1).
 template <int P, int SL, int LAT, bool CL, bool SEG = false>
-__global__ void __launch_bounds__(SEG ? kSegMaxThreads : kResMaxThreads, 1) k_resident(BatchParams p) {
+__global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG>(), 1) k_resident(BatchParams p) {
   extern __shared__ __align__(16) word_t s_spins[];
   __shared__ unsigned s_cnt[2][64];   // this CTA's partial counts
   __shared__ unsigned s_tot[2][64];   // cluster totals
@@ -464,6 +471,44 @@ __global__ void __launch_bounds__(SEG ? kSegMaxThreads : kResMaxThreads, 1) k_re
     my_elast = st->elast[threadIdx.x];
   }
   if (d.sched >= 0) measured = st->measured;
+  // Fused measurement for single-slot 3D anneal instances walked whole: the
+  // energy of a measured sweep is counted inside its colour-1 half and the
+  // next sweep's colour-0 half (rhalf_3d1), then folded; only the last
+  // measurement of a launch needs the separate pass. Each lane's count must
+  // stay below 2048: columns per lane x (6L + 2) bonds, from the largest CTA.
+  constexpr bool FUSE_T = (P == 1 && SL == 1 && LAT == SA_LATTICE_3D && !SEG);
+  bool fuse = false;
+  if constexpr (FUSE_T) {
+    const long cols_max = (long)((d.L + C - 1) / C) * (d.L / 2);
+    const long rounds = (cols_max + blockDim.x - 1) / blockDim.x;
+    fuse = d.sched >= 0 && p.mstride > 0 && d.L > 4 && rounds * (6L * d.L + 2) < 2048;
+  }
+  BondCount bc;
+  bc.clear();
+  bool pending = false;     // a measured sweep whose colour-0 bonds are still to count
+  int64_t rec_step = -1;    // its step, when it ended a step (the per-step record waits for it)
+  // fold the counts in s_cnt (summed over the cluster) into the anneal record
+  auto fold_counts = [&]() {
+    sync_all();
+    if (threadIdx.x < 64) {
+      unsigned v = 0;
+      if (CL) {
+        for (int r = 0; r < C; ++r) v += cluster.map_shared_rank(&s_cnt[0][0], (unsigned)r)[threadIdx.x];
+      } else {
+        v = s_cnt[0][threadIdx.x];
+      }
+      if (q == 0) {
+        const int64_t e = 2 * (int64_t)v - d.nbonds;
+        my_elast = e;
+        my_emax = (measured == 0) ? e : max(my_emax, e);
+        if (rec_step >= 0 && p.step_rec && rec_step < d.thr_count)
+          p.step_rec[((int64_t)d.state_idx * d.thr_count + rec_step) * 64 + threadIdx.x] = e;
+      }
+    }
+    measured += 1;
+    rec_step = -1;
+    sync_all();  // every CTA has read s_cnt before it is cleared again
+  };
   __syncthreads();
   for (int64_t i = 0; i < n; ++i) {
     // this sweep's exchange decision, fetched before the half-sweeps hide its latency
@@ -482,15 +527,35 @@ __global__ void __launch_bounds__(SEG ? kSegMaxThreads : kResMaxThreads, 1) k_re
           for (int k = 0; k < 8; ++k) { th[q][k] = t->dn[k]; tb[q][k] = t->bdn[k]; }
       }
     }
+    const bool meas_now = d.sched >= 0 && p.mstride > 0 && (sweeps % d.sweeps_per_step) % p.mstride == 0;
     for (int c = 0; c < 2; ++c) {
+      if (fuse && c == 0 && pending)
+        for (int t = threadIdx.x; t < 128; t += blockDim.x) (&s_cnt[0][0])[t] = 0;
       if (d3) {
         if constexpr (SEG) {
           rhalf_3d1s<CL>(x, c, draw + c, th[0]);
-        } else if (P == 1 && SL == 1 && x.L > 4) rhalf_3d1<2, CL>(x, c, draw + c, th[0]);
-        else rhalf_3d<P, SL, CL>(x, c, draw + c, th);
+        } else if (P == 1 && SL == 1 && x.L > 4) {
+          const int cmode = !fuse ? 0 : (c == 0 ? (pending ? 1 : 0) : (meas_now ? 2 : 0));
+          rhalf_3d1<2, CL>(x, c, draw + c, th[0], &bc, cmode);
+        } else {
+          rhalf_3d<P, SL, CL>(x, c, draw + c, th);
+        }
       }
       else rhalf_2d<P, SL, open, CL>(x, c, draw + c, th, tb);
       sync_all();
+      if (fuse && c == 0 && pending) {
+        // the previous sweep's count is complete: reduce it over the CTA
+        bc.flush();
+        VCount<16> w;
+#pragma unroll
+        for (int b = 0; b < 16; ++b) w.p[b] = (b < 11) ? bc.big.p[b] : 0;
+        w.warp_sum_from(1);
+        atomicAdd(&s_cnt[0][lane], w.count_of(lane));
+        atomicAdd(&s_cnt[0][lane + 32], w.count_of(lane + 32));
+        bc.clear();
+        fold_counts();
+        pending = false;
+      }
     }
     draw += 2;
     const int64_t in_step = (d.sched >= 0) ? sweeps % d.sweeps_per_step : 0;
@@ -516,7 +581,12 @@ __global__ void __launch_bounds__(SEG ? kSegMaxThreads : kResMaxThreads, 1) k_re
         sync_all();
       }
     }
-    const bool meas = d.sched >= 0 && p.mstride > 0 && in_step % p.mstride == 0;
+    bool meas = d.sched >= 0 && p.mstride > 0 && in_step % p.mstride == 0;
+    if (fuse && meas) {
+      pending = true;
+      meas = false;
+      if (sweeps % d.sweeps_per_step == 0) rec_step = sweeps / d.sweeps_per_step - 1;
+    }
     if (xchg || meas) {
       int a = 0, nsl = 1;
       if (xchg) {
@@ -574,10 +644,17 @@ __global__ void __launch_bounds__(SEG ? kSegMaxThreads : kResMaxThreads, 1) k_re
       sync_all();
       if (meas) measured += 1;
     }
-    if (p.step_rec && d.sched >= 0 && q == 0 && threadIdx.x < 64 && sweeps % d.sweeps_per_step == 0) {
+    if (p.step_rec && d.sched >= 0 && q == 0 && threadIdx.x < 64 && sweeps % d.sweeps_per_step == 0 &&
+        !pending) {
       const int64_t stp = sweeps / d.sweeps_per_step - 1;
       if (stp < d.thr_count) p.step_rec[((int64_t)d.state_idx * d.thr_count + stp) * 64 + threadIdx.x] = my_elast;
     }
+  }
+  if (pending) {
+    // the launch's last measured sweep: count its energy with the separate pass
+    rmeasure<CL>(x, d3, open, 0, 1, s_cnt);
+    fold_counts();
+    pending = false;
   }
   // local -> global
   for (int cz = 0; cz < 2 * x.zc; ++cz) {
@@ -918,7 +995,9 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
           }
         }
         const int passes = passes_for(g.RP);
-        int warps = std::min(passes, seg ? kSegMaxThreads / 32 : kResMaxWarps);
+        const bool big_regs = seg || (d.lattice == SA_LATTICE_3D && g.SL == 1 && g.RP == 1);
+        const int wmax = big_regs ? kSegMaxThreads / 32 : kResMaxWarps;
+        int warps = std::min(passes, wmax);
         const int rounds = (passes + warps - 1) / warps;
         warps = std::max(4, (passes + rounds - 1) / rounds);
         if (d.nslots == 1 && smem >= 64 * 1024) {
@@ -926,7 +1005,7 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
           // every sweep: give the measurement pass (one unit = 32 sites of one
           // colour and plane) at least ~4 units per warp of parallelism
           const int units = 2 * ((d.lattice == SA_LATTICE_3D) ? d.L : 1) * ((ny * hL + 31) / 32);
-          warps = std::max(warps, std::min(seg ? kSegMaxThreads / 32 : kResMaxWarps, (units + 3) / 4));
+          warps = std::max(warps, std::min(wmax, (units + 3) / 4));
         }
         g.threads = warps * 32;
       }

@@ -405,6 +405,53 @@ __device__ __forceinline__ word_t below(word_t c0, word_t c1, word_t c2, uint32_
   return (word_t)r[0] | ((word_t)r[1] << 32);
 }
 
+// Per-lane satisfied-bond counter of the fused single-slot measurement: a
+// 5-plane counter (values < 32) that takes adds of at most 5 and flushes into
+// an 11-plane one before it could overflow. A lane's count over one measured
+// sweep stays below 2048 (the kernel checks the bound before fusing).
+struct BondCount {
+  VCount<5> sm;
+  VCount<11> big;
+  int cap;  // largest value sm can hold now
+  __device__ __forceinline__ void clear() {
+    sm.clear();
+    big.clear();
+    cap = 0;
+  }
+  __device__ __forceinline__ void flush() {
+    word_t carry = 0;
+#pragma unroll
+    for (int b = 0; b < 11; ++b) {
+      const word_t q = (b < 5) ? sm.p[b] : 0;
+      const word_t a = big.p[b];
+      big.p[b] = a ^ q ^ carry;
+      carry = (a & q) | (carry & (a ^ q));
+    }
+    sm.clear();
+    cap = 0;
+  }
+  // += the 3-plane count (q2 q1 q0) <= 5
+  __device__ __forceinline__ void add3(word_t q0, word_t q1, word_t q2) {
+    if (cap + 5 > 31) flush();
+    const word_t s0 = sm.p[0] ^ q0, k0 = sm.p[0] & q0;
+    const word_t t1 = sm.p[1] ^ q1, k1 = (sm.p[1] & q1) | (k0 & t1);
+    const word_t t2 = sm.p[2] ^ q2, k2 = (sm.p[2] & q2) | (k1 & t2);
+    sm.p[0] = s0;
+    sm.p[1] = t1 ^ k0;
+    sm.p[2] = t2 ^ k1;
+    const word_t k3 = sm.p[3] & k2;
+    sm.p[3] ^= k2;
+    sm.p[4] ^= k3;
+    cap += 5;
+  }
+  // += one bond bit
+  __device__ __forceinline__ void add1(word_t q) {
+    if (cap + 1 > 31) flush();
+    sm.add(q);
+    cap += 1;
+  }
+};
+
 // Single-slot 3D half-sweep. Sites of one colour in one (x, y) column depend
 // on each other along z (the colour is (x+y)%2, so a site's z-1 neighbour has
 // its colour and is updated first). The walk is split in two phases per chunk
@@ -418,8 +465,17 @@ __device__ __forceinline__ word_t below(word_t c0, word_t c1, word_t c2, uint32_
 // applies Z maps at two logic operations each. The top plane's z+1
 // neighbour is the new z = 0 spin, known once the first chunk is applied
 // (requires L > Z).
+//
+// Fused measurement (bc != null): -H after a sweep is counted from values the
+// walk already holds, every bond once. cmode 1 (the next sweep's colour-0
+// half, before its updates): each colour-0 site adds its four in-plane bonds
+// (all of them lead to colour 1) and its old bond to z+1, the top plane its
+// in-plane bonds only and the bottom plane the wrapped bond to the old top.
+// cmode 2 (the measured sweep's colour-1 half): each colour-1 site adds its
+// new bond to z-1, the top plane also the new wrapped bond to z = 0.
 template <int Z, bool CL>
-__device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw, const uint32_t* th) {
+__device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw, const uint32_t* th,
+                                          BondCount* bc = nullptr, int cmode = 0) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int L = x.L, hL = x.hL;
   const int cols = x.ny * hL;
@@ -454,13 +510,15 @@ __device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw,
     word_t* own_w = const_cast<word_t*>(own);
     word_t prev = own[(L - 1) * zs];  // old top spin: the z-1 neighbour of z = 0
     word_t first = 0;
+    word_t jlast = 0;  // coupling of the wrapped bond (L-1, 0)
     for (int z0 = 0; z0 < L; z0 += Z) {
-      word_t A[Z], B[Z];
+      word_t A[Z], B[Z], JU[Z];
 #pragma unroll
       for (int i = 0; i < Z; ++i) {
         const int z = z0 + i;
         A[i] = 0;
         B[i] = 0;
+        JU[i] = 0;
         if (z < L) {
           const bool last = (z == L - 1);
           const int zn = last ? 0 : z + 1;
@@ -485,15 +543,32 @@ __device__ __forceinline__ void rhalf_3d1(const ResCtx& x, int c, uint64_t draw,
           const word_t f0 = (g & hi) | (~g & lo);
           A[i] = si ^ f0;
           B[i] = lo ^ hi;
+          JU[i] = ju;
+          if (last) jlast = jd;
+          if (cmode == 1) {
+            if (!last) {
+              bc->add3(c0, c1, c2);
+            } else {
+              word_t d0, d1, d2;
+              count4(jw ^ sw ^ si, jee ^ se ^ si, jn ^ sn ^ si, jss ^ ss ^ si, d0, d1, d2);
+              bc->add3(d0, d1, d2);
+            }
+            if (z == 0) bc->add1(g ^ prev);  // prev is still the old top spin
+          }
         }
       }
 #pragma unroll
       for (int i = 0; i < Z; ++i) {
         const int z = z0 + i;
         if (z < L) {
-          prev = A[i] ^ (prev & B[i]);
-          own_w[z * zs] = prev;
-          if (z == 0) first = prev;
+          const word_t v = A[i] ^ (prev & B[i]);
+          if (cmode == 2) {
+            if (z > 0) bc->add1(JU[i] ^ prev ^ v);
+            if (z == L - 1) bc->add1(jlast ^ v ^ first);
+          }
+          prev = v;
+          own_w[z * zs] = v;
+          if (z == 0) first = v;
         }
       }
     }

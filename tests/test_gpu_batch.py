@@ -253,3 +253,36 @@ def test_energy_histograms_and_decisions(sab, lat, L, nslots):
         assert np.array_equal(b.histogram(0, s), hist[s]), s
     acc, att = b.acceptance(0)
     assert np.allclose(acc / np.maximum(att, 1) / 64.0, pt.acceptance(), rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("stride", [1, 3])
+def test_fused_single_slot_measurement_full_batch(sab, stride):
+    """Single-slot 3D anneals in a batch too large to spread over extra SMs
+    count each measured sweep's energy inside the half-sweeps (lagged by half a
+    sweep); the running maxima and spins must still match annealing<>."""
+    from simulated_annealing_b200.batch import Batch
+    nsteps, per = 3, 4
+    T0, T1 = 2.8, 0.4
+    Ts = [T0 + (T1 - T0) * k / (nsteps - 1) for k in range(nsteps)]
+    b = Batch()
+    b.set_measure_stride(stride)
+    sch = b.add_schedule(Ts, per)
+    specs = [(O.LAT_3D, 8 if k % 3 else 10, 300 + k) for k in range(96)]
+    for lat, L, s in specs:
+        b.add_instance(lat, L, schedule=sch, seed_J=s, seed=s + 1)
+    b.finalize()
+    b.run(5)
+    b.run(100)
+    b.sync()
+    for i in (0, 1, 2, 47, 95):
+        lat, L, s = specs[i]
+        o = O.OracleSystem(lat, L, mode=O.MODE_PHILOX)
+        o.set_seed(s)
+        o.init_J()
+        o.set_seed(s + 1)
+        o.init_rand()
+        mn, _ = o.anneal(T0, 1, T1, nsteps, per, stride)
+        E, done = b.anneal_result(i)
+        assert done == nsteps * per
+        assert np.array_equal(E.astype(np.float32), mn), i
+        assert np.array_equal(b.spins(i, 0), o.spins()), i
