@@ -315,10 +315,13 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
     SlotWords<SL> prev = {};
     if (valid) prev = ldw<SL>(x.sm + own + (L - 1) * zs);
     SlotWords<SL> first = {};
+    word_t jnext = 0;  // the z-1 coupling of the next plane: this plane's z+1 coupling
     for (int z0 = 0; z0 < L; z0 += P) {
-      // Lane (column cl, i) draws the Philox number and loads the six coupling
+      // Lane (column cl, i) draws the Philox number and loads the coupling
       // words of plane z0+i; the column's P lanes share them by shuffles, so
       // each coupling word is loaded once per site instead of once per slot.
+      // A plane's z-1 coupling is the z+1 coupling of the plane below, so it
+      // is loaded and shared only for z = 0.
       const int zd = z0 + (lane % P);
       uint32_t um = 0;
       word_t bw = 0, be = 0, bn = 0, bs = 0, bu = 0, bd = 0;
@@ -329,10 +332,10 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         be = __ldg(Jxo + je + zo);
         bn = __ldg(Jyc + jo + zo);
         bs = __ldg(Jyo + js + zo);
-        bu = __ldg(Jzc + jo + zo);
+        if (zd == 0) bu = __ldg(Jzc + jo);
         bd = __ldg(Jzc + jo + ((zd == L - 1) ? 0 : zo + zg));
       }
-#pragma unroll 2
+#pragma unroll 4
       for (int zi = 0; zi < P; ++zi) {
         const int z = z0 + zi;
         if (z >= L) break;  // warp-uniform
@@ -343,8 +346,10 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         const word_t je_ = (P == 1) ? be : __shfl_sync(0xffffffffu, be, src);
         const word_t jn = (P == 1) ? bn : __shfl_sync(0xffffffffu, bn, src);
         const word_t js_ = (P == 1) ? bs : __shfl_sync(0xffffffffu, bs, src);
-        const word_t ju = (P == 1) ? bu : __shfl_sync(0xffffffffu, bu, src);
+        word_t ju = jnext;
+        if (z == 0) ju = (P == 1) ? bu : __shfl_sync(0xffffffffu, bu, src);  // warp-uniform
         const word_t jd = (P == 1) ? bd : __shfl_sync(0xffffffffu, bd, src);
+        jnext = jd;
         if (valid) {
           const bool last = (z == L - 1);
           const SlotWords<SL> si = ldw<SL>(x.sm + own);
@@ -710,51 +715,100 @@ __device__ __forceinline__ void rhalf_3d1s(const ResCtx& x, int c, uint64_t draw
   }
 }
 
-// Partial satisfied-bond counts of slots a..a+nsl-1 over this CTA's sites
-// (each bond counted once, from its site towards -x/-y/-z) into cnt[q][j].
-// UNR units are formed before any is added, so their loads are in flight
-// together (used where few warps walk many units: single-slot instances).
-template <bool CL, int UNR = 1>
-__device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, int a, int nsl,
-                                         unsigned (*cnt)[64]) {
-  for (int i = threadIdx.x; i < 128; i += blockDim.x) (&cnt[0][0])[i] = 0;
-  __syncthreads();
+// big += small over the low W planes only (values stay below 2^W).
+template <int W>
+__device__ __forceinline__ void add_small_w(VCount<16>& big, const VCount<4>& sm) {
+  word_t carry = 0;
+#pragma unroll
+  for (int b = 0; b < W; ++b) {
+    const word_t q = (b < 4) ? sm.p[b] : 0;
+    const word_t a = big.p[b];
+    big.p[b] = a ^ q ^ carry;
+    carry = (a & q) | (carry & (a ^ q));
+  }
+}
+
+// Sum over the lanes that share (lane mod NSL) of counters below 2^W0 per
+// lane: level l of the butterfly adds values below 2^(W0+l), so it touches
+// W0+l+1 planes (capped at 16) instead of all of them.
+template <int NSL, int W0>
+__device__ __forceinline__ void warp_sum_grow(VCount<16>& v) {
+  constexpr int NL = (NSL == 1) ? 5 : (NSL == 2) ? 4 : 3;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const int off = 16 >> l;
+    word_t carry = 0;
+#pragma unroll
+    for (int b = 0; b < 16; ++b) {
+      if (b < W0 + l + 1) {
+        const word_t a = v.p[b];
+        const word_t q = __shfl_xor_sync(0xffffffffu, a, off);
+        v.p[b] = a ^ q ^ carry;
+        carry = (a & q) | (carry & (a ^ q));
+      }
+    }
+  }
+}
+
+// Partial satisfied-bond counts of slots a..a+NSL-1 over this CTA's sites
+// (each bond counted once, from its site towards -x/-y/-z), added into
+// cnt[q][j]. Lanes: NSL per site, 32/NSL sites per warp row. A unit is one
+// warp row of sites in one (colour, z) plane; units are ordered (row tile,
+// colour, z), so a warp re-derives a site's indices only when it enters a
+// new (tile, colour) and otherwise steps by one plane. A lane counts into W0
+// bit planes; after at most (2^W0 - 1) / bonds-per-site units the warp sums
+// its lanes and adds the totals to cnt. UNR units are formed before any is
+// added, so their loads are in flight together.
+template <bool CL, int UNR, int NSL, int W0>
+__device__ __forceinline__ void rmeasure_body(const ResCtx& x, bool d3, bool open, int a, unsigned (*cnt)[64]) {
+  static_assert(W0 >= 5 && W0 <= 11, "counter width: chunks of at least one UNR round");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int per = 32 / nsl;
-  const int g = lane / nsl, slot = a + lane % nsl;
-  const int L = x.L, hL = x.hL, ns = x.ns;
-  const int cols = x.ny * hL;          // per colour per z
-  VCount<4> sm4;
-  VCount<16> big;
-  sm4.clear();
-  big.clear();
-  const int tiles = (cols + per - 1) / per;      // site tiles per (colour, z)
-  const int units = 2 * x.zc * tiles;
-  // warp w takes the contiguous units [u0, u1) and walks (cz, tile) without division
+  constexpr int per = 32 / NSL;
+  const int g = lane / NSL, slot = a + lane % NSL;
+  const int L = x.L, hL = x.hL, ns = x.ns, zc = x.zc;
+  const int cols = x.ny * hL;
+  const int tiles = (cols + per - 1) / per;
+  const int units = 2 * zc * tiles;
+  const int zs = x.ny * x.rowW, zg = L * hL;
   const int u0 = (int)(((long)units * warp) / nwarps), u1 = (int)(((long)units * (warp + 1)) / nwarps);
-  int cz = u0 / tiles, tile = u0 - cz * tiles;
-  // satisfied-bond bits (q1 q0 = 0..3) of this lane's site in unit (cz, tile)
-  auto unit_bits = [&](int cz_, int tile_, word_t& q0, word_t& q1) {
-    q0 = q1 = 0;
-    const int col = tile_ * per + g;
-    if (col >= cols) return;
-    const int c = (cz_ >= x.zc) ? 1 : 0, z = cz_ - c * x.zc;
-    const int yl = div_hl(col, x);
-    const int k = col - yl * hL, y = x.y0 + yl;
+  const int chunk = ((1 << W0) - 1) / (d3 ? 3 : 2);  // units per lane before a warp sum
+  // the lane's site in the current (tile, colour): plane-0 offsets and strides
+  int tcol = u0 / zc, z = u0 - tcol * zc;
+  bool ok = false, wopen = false;
+  int own0 = 0, w0 = 0, zsn = zs, jr0 = 0;
+  const word_t* Jc = x.J;  // couplings of the site's colour; axis a at Jc + 2*a*half
+  NbRow<CL> pn;
+  auto enter = [&]() {
+    const int tile = tcol >> 1, c = tcol & 1, oc = 1 - c;
+    const int col = tile * per + g;
+    ok = col < cols;
+    const int cc = ok ? col : 0;
+    const int yl = div_hl(cc, x);
+    const int k = cc - yl * hL, y = x.y0 + yl;
     const int par = (c + y) & 1, xx = 2 * k + par;
     int kw, ke;
     x_neighbours(k, par, hL, kw, ke);
-    const int oc = 1 - c;
     const int sk = slot ^ swz(x, k);
-    const word_t si = x.sm[lrow(x, c, z, yl) + k * ns + sk];
-    const long jr = (long)(y + L * z) * hL + k;
-    const word_t w = (open && xx == 0) ? 0 : (__ldg(x.J + (long)(0 + c) * x.half + jr) ^ si ^
-                                               x.sm[lrow(x, oc, z, yl) + kw * ns + (slot ^ swz(x, kw))]);
-    const NbRow<CL> pn = north_row<CL>(x, oc, z, yl);
-    const word_t n = __ldg(x.J + (long)(2 + c) * x.half + jr) ^ si ^ pn.template ld<1>(k * ns + sk).w[0];
+    own0 = lrow(x, c, 0, yl) + k * ns + sk;
+    w0 = lrow(x, oc, 0, yl) + kw * ns + (slot ^ swz(x, kw));
+    pn = north_row<CL>(x, oc, 0, yl);
+    pn.step(k * ns + sk);
+    zsn = (yl > 0) ? zs : x.nyN * x.rowW;
+    jr0 = y * hL + k;
+    Jc = x.J + (long)c * x.half;
+    wopen = open && xx == 0;
+  };
+  // satisfied-bond bits (q1 q0 = 0..3) of this lane's site in plane z
+  auto unit_bits = [&](word_t& q0, word_t& q1) {
+    q0 = q1 = 0;
+    if (!ok) return;
+    const word_t* jp = Jc + (jr0 + z * zg);
+    const word_t si = x.sm[own0 + z * zs];
+    const word_t w = wopen ? 0 : (__ldg(jp) ^ si ^ x.sm[w0 + z * zs]);
+    const word_t n = __ldg(jp + 2 * x.half) ^ si ^ pn.template ld<1>(z * zsn).w[0];
     if (d3) {
       const int zu = (z == 0) ? L - 1 : z - 1;
-      const word_t uu = __ldg(x.J + (long)(4 + c) * x.half + jr) ^ si ^ x.sm[lrow(x, c, zu, yl) + k * ns + sk];
+      const word_t uu = __ldg(jp + 4 * x.half) ^ si ^ x.sm[own0 + zu * zs];
       q0 = w ^ n ^ uu;
       q1 = (w & n) | (uu & (w ^ n));
     } else {
@@ -763,47 +817,70 @@ __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, in
     }
   };
   auto advance = [&]() {
-    if (++tile == tiles) {
-      tile = 0;
-      ++cz;
+    if (++z == zc) {
+      z = 0;
+      ++tcol;
+      enter();
     }
   };
-  int un = u0;
-  if (UNR > 1) {
-    // UNR <= 5 units of <= 3 bonds per round keep the small counter below 16
-    static_assert(UNR <= 5, "small counter range");
-    for (; un + UNR <= u1; un += UNR) {
-      word_t b0[UNR], b1[UNR];
+  if (u0 < u1) enter();
+  const int q = lane % NSL;
+  for (int un = u0; un < u1;) {  // warp-uniform
+    const int ue = min(u1, un + chunk);
+    VCount<4> sm4;
+    VCount<16> big;
+    sm4.clear();
+    big.clear();
+    if (UNR > 1) {
+      // UNR <= 5 units of <= 3 bonds per round keep the small counter below 16
+      static_assert(UNR <= 5, "small counter range");
+      for (; un + UNR <= ue; un += UNR) {
+        word_t b0[UNR], b1[UNR];
 #pragma unroll
-      for (int i = 0; i < UNR; ++i) {
-        unit_bits(cz, tile, b0[i], b1[i]);
-        advance();
+        for (int i = 0; i < UNR; ++i) {
+          unit_bits(b0[i], b1[i]);
+          advance();
+        }
+#pragma unroll
+        for (int i = 0; i < UNR; ++i) add2_small(sm4, b0[i], b1[i]);
+        add_small_w<W0>(big, sm4);
+        sm4.clear();
       }
+    }
+    int it = 0;
+    for (; un < ue; ++un) {
+      word_t b0, b1;
+      unit_bits(b0, b1);
+      add2_small(sm4, b0, b1);
+      advance();
+      if (++it == 5) {
+        add_small_w<W0>(big, sm4);
+        sm4.clear();
+        it = 0;
+      }
+    }
+    add_small_w<W0>(big, sm4);
+    warp_sum_grow<NSL, W0>(big);
 #pragma unroll
-      for (int i = 0; i < UNR; ++i) add2_small(sm4, b0[i], b1[i]);
-      add_small(big, sm4);
-      sm4.clear();
+    for (int m = 0; m < 2 * NSL; ++m) {
+      const int j = (lane / NSL) + per * m;
+      atomicAdd(&cnt[q][j], big.count_of(j));
     }
   }
-  int it = 0;
-  for (; un < u1; ++un) {
-    word_t b0, b1;
-    unit_bits(cz, tile, b0, b1);
-    add2_small(sm4, b0, b1);
-    advance();
-    if (++it == 5) {
-      add_small(big, sm4);
-      sm4.clear();
-      it = 0;
-    }
-  }
-  add_small(big, sm4);
-  big.warp_sum_from(nsl);
-  const int q = lane % nsl;
-  for (int m = 0; m < 2 * nsl; ++m) {
-    const int j = (lane / nsl) + per * m;
-    atomicAdd(&cnt[q][j], big.count_of(j));
-  }
+}
+
+// Partial satisfied-bond counts of slots a..a+nsl-1 (nsl 1 or 2) over this
+// CTA's sites into cnt[q][j] (zeroed here). Five counter planes per lane: a
+// batched ensemble's share of a warp fits in one chunk (one warp sum per
+// measurement); a single-slot lattice spread over few warps takes a warp
+// sum every 10 (3D) or 15 (2D) units, which keeps the counters in registers.
+template <bool CL, int UNR = 1>
+__device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, int a, int nsl,
+                                         unsigned (*cnt)[64]) {
+  for (int i = threadIdx.x; i < 128; i += blockDim.x) (&cnt[0][0])[i] = 0;
+  __syncthreads();
+  if (nsl == 2) rmeasure_body<CL, UNR, 2, 5>(x, d3, open, a, cnt);
+  else rmeasure_body<CL, UNR, 1, 5>(x, d3, open, a, cnt);
 }
 
 }  // namespace sa
