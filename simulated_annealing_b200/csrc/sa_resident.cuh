@@ -179,8 +179,13 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
                                          const uint32_t (*tb)[8]) {
   constexpr int SPS = 32 / P;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int slot = (lane % P) * SL;
-  const bool slot_ok = slot < x.ns;
+  // Clustered instances (BF): a lane without a slot (or a site) updates
+  // slot 0 (site 0) of the CTA, reading only, and drops its store, so the
+  // update has no divergent branch (measured faster there, and slower for
+  // single-CTA instances).
+  constexpr bool BF = CL;
+  const bool slot_ok = (lane % P) * SL < x.ns;
+  const int slot = (BF && !slot_ok) ? 0 : (lane % P) * SL;
   const int tot = x.ny * x.hL;
   const int L = x.L, hL = x.hL, ns = x.ns;
   const int oc = 1 - c;
@@ -193,11 +198,12 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
     // coupling words, its row offsets, its neighbours' swizzles and its border
     // flags. The P lanes updating that site's slots fetch them by shuffles
     // instead of each recomputing the indices and reloading the couplings.
-    const int my = base + lane;
+    const bool have = base + lane < tot;
+    const int my = (BF && !have) ? 0 : base + lane;
     uint32_t um = 0, pk = 0, nadr = 0, sadr = 0;
     int rowc = 0, roww = 0, rowe = 0;
     word_t bw = 0, be = 0, bn = 0, bs = 0;
-    if (my < tot) {
+    if (BF || have) {
       const int yl = div_hl(my, x);
       const int k = my - yl * hL, y = x.y0 + yl;
       const int par = (c + y) & 1, xx = 2 * k + par;
@@ -234,7 +240,8 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
       const int rc = share(rowc), rw = share(roww), re = share(rowe);
       const uint32_t f = share(pk), na = share(nadr), sa = share(sadr);
       const int t = base + sl;
-      if (t < tot && slot_ok) {
+      const bool upd = t < tot && slot_ok;
+      if (BF || upd) {
         const int sk = slot ^ (int)(f & 0xFFu);
         const int own = rc + sk;
         const SlotWords<SL> si = ldw<SL>(x.sm + own);
@@ -268,7 +275,7 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
           prefix_bits(u, border ? tb[q] : th[q], m0, m1, m2);
           out.w[q] = flip_below(si.w[q], c0, c1, c2, m0, m1, m2);
         }
-        stw<SL>(x.sm + own, out);
+        if (!BF || upd) stw<SL>(x.sm + own, out);
       }
     }
   }
@@ -315,16 +322,16 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
     SlotWords<SL> prev = {};
     if (valid) prev = ldw<SL>(x.sm + own + (L - 1) * zs);
     SlotWords<SL> first = {};
-    word_t jnext = 0;  // the z-1 coupling of the next plane: this plane's z+1 coupling
+    word_t jnext = __ldg(Jzc + jo);  // the z-1 coupling of the next plane (plane 0: the wrapped bond)
     for (int z0 = 0; z0 < L; z0 += P) {
       // Lane (column cl, i) draws the Philox number and loads the coupling
       // words of plane z0+i; the column's P lanes share them by shuffles, so
       // each coupling word is loaded once per site instead of once per slot.
-      // A plane's z-1 coupling is the z+1 coupling of the plane below, so it
-      // is loaded and shared only for z = 0.
+      // A plane's z-1 coupling is the z+1 coupling of the plane below; plane
+      // 0's (the wrapped bond) every lane loads before the walk.
       const int zd = z0 + (lane % P);
       uint32_t um = 0;
-      word_t bw = 0, be = 0, bn = 0, bs = 0, bu = 0, bd = 0;
+      word_t bw = 0, be = 0, bn = 0, bs = 0, bd = 0;
       if (col_ok && zd < L) {
         um = philox_draw(x.seed, (unsigned long long)(xx + L * (y + L * zd)), draw);
         const int zo = zd * zg;
@@ -332,7 +339,6 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         be = __ldg(Jxo + je + zo);
         bn = __ldg(Jyc + jo + zo);
         bs = __ldg(Jyo + js + zo);
-        if (zd == 0) bu = __ldg(Jzc + jo);
         bd = __ldg(Jzc + jo + ((zd == L - 1) ? 0 : zo + zg));
       }
 #pragma unroll 4
@@ -346,8 +352,7 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         const word_t je_ = (P == 1) ? be : __shfl_sync(0xffffffffu, be, src);
         const word_t jn = (P == 1) ? bn : __shfl_sync(0xffffffffu, bn, src);
         const word_t js_ = (P == 1) ? bs : __shfl_sync(0xffffffffu, bs, src);
-        word_t ju = jnext;
-        if (z == 0) ju = (P == 1) ? bu : __shfl_sync(0xffffffffu, bu, src);  // warp-uniform
+        const word_t ju = jnext;
         const word_t jd = (P == 1) ? bd : __shfl_sync(0xffffffffu, bd, src);
         jnext = jd;
         if (valid) {
