@@ -34,6 +34,7 @@
 #include "sa_host.hpp"
 #include "sa_resident.cuh"
 #include "sa_system.hpp"
+#include "sa_wide.cuh"
 
 namespace sa {
 
@@ -810,6 +811,7 @@ struct sa_batch {
   uint64_t* d_seedJ = nullptr; // serving: seeds of the requests being initialised
   int64_t e_count = 0;         // sum of nslots*64
   bool force_global = false;   // run every instance in the global-memory kernel
+  bool no_wide = false;        // never run an instance wide (sa_wide.cuh)
   int hstride = 0;             // energy histograms every hstride sweeps (0 = off)
   int32_t* d_hist = nullptr;
   int64_t hist_count = 0;
@@ -823,6 +825,9 @@ struct sa_batch {
     int lattice, L;     // resident groups hold one shape each
     int SL, RP;         // resident: slots per lane and lanes per site
     bool seg;           // resident: single-slot 3D walked in column segments
+    bool wide;          // one single-slot 3D anneal spread over the whole GPU (sa_wide.cuh)
+    int wide_id;        // wide: the instance
+    int wide_slot;      // wide: its scratch block in d_wide
     cudaStream_t stream;
     cudaEvent_t done;
   };
@@ -830,7 +835,36 @@ struct sa_batch {
   cudaEvent_t fork = nullptr;
   std::vector<int> cluster_of;  // per instance: C (0 = global-memory kernel)
   bool spread = false;          // clusters were enlarged to use idle SMs
+  std::vector<int64_t> run_start;  // per instance: sweeps done when the current run began
+  char* d_wide = nullptr;          // scratch of the wide groups, kWideScratch bytes each
+  int wide_cap = 0;                // wide groups the scratch holds
+  // CUDA graphs of kWideGraphSweeps wide sweeps, by launch parameters
+  struct WideGraph {
+    WideParams wp;
+    unsigned hgrid, egrid;
+    cudaGraphExec_t exec;
+  };
+  std::vector<WideGraph> wide_graphs;  // destroyed with the batch, after its streams are idle
+  sa_batch() = default;
+  sa_batch(const sa_batch&) = delete;
+  sa_batch& operator=(const sa_batch&) = delete;
+  ~sa_batch() {
+    for (auto& w : wide_graphs) cudaGraphExecDestroy(w.exec);
+  }
 };
+
+// Per wide group: 64 bond counters, the ticket, the end sweep.
+constexpr size_t kWideScratch = 512;
+// Sweeps per CUDA graph of the wide form (three kernel nodes each); a run
+// replays it and launches the remainder directly.
+constexpr int kWideGraphSweeps = 25;
+// 3D L from which a single-slot anneal runs wide: always from kWideMinL (its
+// resident walk is latency-bound even in a full batch: L=48 50.7 -> 29 us per
+// sweep, L=64 98.9 -> 35.7), and from kWideSpreadL when the batch is spread
+// (below it the segmented resident walk on one cluster is faster: L=32 15.3
+// against 22.1 us per sweep).
+constexpr int kWideMinL = 48;
+constexpr int kWideSpreadL = 40;
 
 // Shared-memory budget of one CTA of the resident kernel: the 227 KB opt-in
 // limit minus room for its static arrays (counters, per-warp planes).
@@ -951,17 +985,24 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
     // chained walk is latency-bound; beyond that it is throughput-bound and the
     // segments' extra map and scan work costs more than it saves (measured:
     // 3D L=32 on 16 CTAs 49.8 -> 17.2 us per sweep, L=64 97.6 -> 136.7).
-    bool seg = C != 0 && b->spread && d.lattice == SA_LATTICE_3D && d.nslots == 1 && d.L > 4;
+    // A lone single-slot 3D anneal of L >= kWideMinL leaves even a 16-CTA
+    // cluster latency-bound; it runs wide, over the whole GPU.
+    const bool wide = C != 0 && d.lattice == SA_LATTICE_3D && d.nslots == 1 && d.sched >= 0 && !b->no_wide &&
+                      (d.L >= kWideMinL || (b->spread && d.L >= kWideSpreadL));
+    bool seg = C != 0 && b->spread && d.lattice == SA_LATTICE_3D && d.nslots == 1 && d.L > 4 && !wide;
     if (seg) {
       const long lanes = (long)((d.L + C - 1) / C) * (d.L / 2) * seg_lanes(d.L);
       seg = (lanes + kSegMaxThreads - 1) / kSegMaxThreads <= 3;
     }
-    const bool same = !b->groups.empty() && b->groups.back().resident == (C != 0) && b->groups.back().P == d.P &&
+    const bool same = !wide && !b->groups.empty() && !b->groups.back().wide &&
+                      b->groups.back().resident == (C != 0) && b->groups.back().P == d.P &&
                       b->groups.back().C == C && b->groups.back().seg == seg &&
                       (C == 0 || (b->groups.back().lattice == d.lattice && b->groups.back().L == d.L));
     if (!same) {
       sa_batch::Group g{};
-      g.resident = C != 0;
+      g.resident = C != 0 && !wide;
+      g.wide = wide;
+      g.wide_id = wide ? order[i] : -1;
       g.P = d.P;
       g.C = C;
       g.begin = (int)i;
@@ -971,7 +1012,7 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
       g.SL = 1;
       g.RP = d.P;
       g.seg = seg;
-      if (C) {
+      if (C && !wide) {
         // warp passes of one half-sweep: 3D walks columns, 32/RP per pass; 2D
         // takes tiles of 32 sites (RP sub-steps of 32/RP sites each). Two slots
         // per lane (16-byte accesses, shared addressing and couplings) when the
@@ -1013,9 +1054,102 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
     }
     sa_batch::Group& g = b->groups.back();
     g.count += 1;
-    g.smem = std::max(g.smem, smem);
+    if (!wide) g.smem = std::max(g.smem, smem);
   }
+  int nw = 0;
+  for (auto& g : b->groups)
+    if (g.wide) g.wide_slot = nw++;
   return order;
+}
+
+// Scratch for the wide groups of the current table (zeroed when allocated;
+// the launches leave it zeroed after every sweep).
+static int ensure_wide_scratch(sa_batch* b) {
+  int nw = 0;
+  for (const auto& g : b->groups) nw += g.wide ? 1 : 0;
+  if (nw <= b->wide_cap) return SA_OK;
+  SA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  cudaFree(b->d_wide);
+  b->d_wide = nullptr;
+  b->wide_cap = std::max(nw, 2 * b->wide_cap);
+  SA_CUDA_TRY(cudaMalloc(&b->d_wide, (size_t)b->wide_cap * kWideScratch));
+  SA_CUDA_TRY(cudaMemsetAsync(b->d_wide, 0, (size_t)b->wide_cap * kWideScratch, b->stream));
+  return SA_OK;
+}
+
+// The sweeps of this run for a wide group: three launches per sweep on the
+// group's stream (the two half-sweeps and the end-of-sweep measurement).
+static int launch_wide(sa_batch* b, const sa_batch::Group& g, long nsweeps, int64_t* step_rec) {
+  const int id = g.wide_id;
+  const InstDesc& d = b->inst[id];
+  const int64_t start = (id < (int)b->run_start.size()) ? b->run_start[id] : 0;
+  int64_t end = start + nsweeps;
+  if (d.sweep_limit >= 0) end = std::min<int64_t>(end, d.sweep_limit);
+  if (end <= start) return SA_OK;
+  char* scratch = b->d_wide + (size_t)g.wide_slot * kWideScratch;
+  WideParams wp;
+  wp.inst = b->d_inst;
+  wp.state = b->d_state;
+  wp.id = id;
+  wp.mstride = b->mstride;
+  wp.spins = b->d_spins;
+  wp.J = b->d_J;
+  wp.thr = b->d_thr;
+  wp.step_rec = step_rec;
+  wp.cnt = reinterpret_cast<unsigned*>(scratch);
+  wp.ticket = reinterpret_cast<unsigned*>(scratch + 256);
+  int64_t* d_end = reinterpret_cast<int64_t*>(scratch + 264);
+  wp.end = d_end;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  const long threads = (long)d.L * (d.L / 2) * wide_lanes(d.L);
+  const unsigned hgrid = (unsigned)((threads + kWideThreads - 1) / kWideThreads);
+  // end-of-sweep grid: one block per SM (few atomics per counter), and enough
+  // threads that none counts more than 10 sites (its bond count stays below 32)
+  const long egrid = std::max<long>(std::min<long>((d.N + kWideThreads - 1) / kWideThreads, (long)sms),
+                                    (d.N + 10L * kWideThreads - 1) / (10L * kWideThreads));
+  k_wide_set_end<<<1, 1, 0, g.stream>>>(d_end, end);
+  SA_CUDA_TRY(cudaGetLastError());
+  auto sweeps = [&](int64_t n) {
+    for (int64_t i = 0; i < n; ++i) {
+      k_wide_half<<<hgrid, kWideThreads, 0, g.stream>>>(wp, 0);
+      k_wide_half<<<hgrid, kWideThreads, 0, g.stream>>>(wp, 1);
+      k_wide_end<<<(unsigned)egrid, kWideThreads, 0, g.stream>>>(wp);
+    }
+  };
+  int64_t n = end - start;
+  if (n >= kWideGraphSweeps) {
+    // the launch sequence of a sweep never changes (the sweep counter, draw
+    // index and thresholds live in device memory): replay a captured graph
+    cudaGraphExec_t exec = nullptr;
+    for (const auto& w : b->wide_graphs)
+      if (w.hgrid == hgrid && w.egrid == (unsigned)egrid && memcmp(&w.wp, &wp, sizeof wp) == 0) exec = w.exec;
+    if (!exec) {
+      cudaGraph_t graph = nullptr;
+      if (cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+        sweeps(kWideGraphSweeps);
+        if (cudaStreamEndCapture(g.stream, &graph) == cudaSuccess && graph) {
+          if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) exec = nullptr;
+          cudaGraphDestroy(graph);
+        }
+      }
+      cudaGetLastError();  // a stream that cannot be captured: launch directly
+      if (exec) {
+        sa_batch::WideGraph w;
+        memcpy(&w.wp, &wp, sizeof wp);
+        w.hgrid = hgrid;
+        w.egrid = (unsigned)egrid;
+        w.exec = exec;
+        b->wide_graphs.push_back(w);
+      }
+    }
+    if (exec) {
+      for (; n >= kWideGraphSweeps; n -= kWideGraphSweeps) SA_CUDA_TRY(cudaGraphLaunch(exec, g.stream));
+    }
+  }
+  sweeps(n);
+  SA_CUDA_TRY(cudaGetLastError());
+  return SA_OK;
 }
 
 // Extends every ladder's exchange table to cover `need` attempts. Each
@@ -1121,6 +1255,7 @@ static int launch_group(sa_batch* b, const sa_batch::Group& g, int gi, long nswe
   p.order = b->d_order + g.begin;
   p.ninst = g.count;
   p.work = b->d_work + gi;
+  if (g.wide) return launch_wide(b, g, nsweeps, nullptr);
   if (!g.resident) {
     k_batch<P><<<g.grid, kBatchThreads, 0, g.stream>>>(p);
     SA_CUDA_TRY(cudaGetLastError());
@@ -1262,6 +1397,7 @@ int sa_batch_destroy(sa_batch_t b) {
   cudaFree(b->d_Eall);
   cudaFree(b->d_hist);
   cudaFree(b->d_seedJ);
+  cudaFree(b->d_wide);
   for (auto& g : b->groups) {
     if (g.stream) cudaStreamDestroy(g.stream);
     if (g.done) cudaEventDestroy(g.done);
@@ -1391,6 +1527,7 @@ int sa_batch_finalize(sa_batch_t b) {
     SA_CUDA_TRY(cudaMemsetAsync(b->d_hist, 0, b->hist_count * sizeof(int32_t), b->stream));
   }
   std::vector<int32_t> order = build_groups(b);
+  if (int st = ensure_wide_scratch(b)) return st;
   const size_t ni = b->inst.size();
   SA_CUDA_TRY(cudaMalloc(&b->d_inst, ni * sizeof(InstDesc)));
   SA_CUDA_TRY(cudaMalloc(&b->d_state, ni * sizeof(InstState)));
@@ -1474,9 +1611,11 @@ int sa_batch_histogram(sa_batch_t b, int id, int slot, int32_t* out, long cap, l
 }
 
 int sa_batch_set_kernel(sa_batch_t b, int kernel) {
-  if (!b || kernel < 0 || kernel > 1) return fail(SA_ERR_INVALID, "kernel must be 0 (auto) or 1 (global)");
+  if (!b || kernel < 0 || kernel > 2)
+    return fail(SA_ERR_INVALID, "kernel must be 0 (auto), 1 (global) or 2 (auto without the wide form)");
   if (b->finalized) return fail(SA_ERR_INVALID, "choose the kernel before finalize");
   b->force_global = (kernel == 1);
+  b->no_wide = (kernel == 2);
   return SA_OK;
 }
 
@@ -1517,6 +1656,7 @@ int sa_batch_run(sa_batch_t b, long nsweeps) {
   if (nsweeps < 0) return fail(SA_ERR_INVALID, "nsweeps < 0");
   if (nsweeps == 0) return SA_OK;
   // host mirror of the counters -> exchange-table lengths this launch needs
+  b->run_start = b->h_sweeps;
   std::vector<int64_t> need(b->ladders.size(), 0);
   for (size_t i = 0; i < b->inst.size(); ++i) {
     const InstDesc& d = b->inst[i];
@@ -1888,6 +2028,8 @@ int sa_serve_destroy(sa_serve_t s) {
   cudaFree(b.d_inst);
   cudaFree(b.d_order);
   cudaFree(b.d_work);
+  cudaFree(b.d_wide);
+  b.d_wide = nullptr;
   b.d_spins = b.d_J = nullptr;
   b.d_thr = nullptr;
   b.d_state = nullptr;
@@ -1986,8 +2128,12 @@ int sa_serve_run(sa_serve_t s, long nsweeps) {
       kv.second.fresh = false;
     }
   b.inst.clear();
+  b.run_start.clear();
   for (auto& kv : s->active)
-    if (kv.second.sweeps < kv.second.d.sweep_limit) b.inst.push_back(kv.second.d);
+    if (kv.second.sweeps < kv.second.d.sweep_limit) {
+      b.inst.push_back(kv.second.d);
+      b.run_start.push_back(kv.second.sweeps);
+    }
   const size_t ni = b.inst.size();
   const size_t need = std::max(ni, fresh.size());
   if (need > b.inst_cap) {
@@ -2011,6 +2157,7 @@ int sa_serve_run(sa_serve_t s, long nsweeps) {
   }
   if (ni == 0) return SA_OK;
   std::vector<int32_t> order = build_groups(&b);
+  if (int st = ensure_wide_scratch(&b)) return st;
   if (b.groups.size() > b.work_cap) {
     SA_CUDA_TRY(cudaStreamSynchronize(b.stream));
     cudaFree(b.d_work);
@@ -2166,14 +2313,15 @@ int resident_run(sa_system* sy, const double* T, int nsteps, int sweeps, int str
   d.sweep_limit = (int64_t)nsteps * sweeps;
   tmp.inst.push_back(d);
   std::vector<int32_t> order = build_groups(&tmp);
-  if (tmp.groups.size() != 1 || !tmp.groups[0].resident)
+  if (tmp.groups.size() != 1 || !(tmp.groups[0].resident || tmp.groups[0].wide))
     return fail(SA_ERR_UNSUPPORTED, "lattice does not fit a cluster's shared memory");
   // one device block: descriptor, state, order, work counter, pair counters,
-  // thresholds, per-step record
+  // thresholds, per-step record, wide-form scratch
   const size_t o_state = 256, o_order = o_state + ((sizeof(InstState) + 255) / 256) * 256;
   const size_t o_work = o_order + 256, o_acc = o_work + 256, o_thr = o_acc + 256;
   const size_t o_rec = o_thr + ((nsteps * sizeof(BThr) + 255) / 256) * 256;
-  const size_t bytes = o_rec + (size_t)nsteps * 64 * sizeof(int64_t);
+  const size_t o_wide = o_rec + (((size_t)nsteps * 64 * sizeof(int64_t) + 255) / 256) * 256;
+  const size_t bytes = o_wide + kWideScratch;
   char* blk = nullptr;
   SA_CUDA_TRY(cudaMalloc(&blk, bytes));
   auto release = [&]() { cudaFree(blk); };
@@ -2197,6 +2345,7 @@ int resident_run(sa_system* sy, const double* T, int nsteps, int sweeps, int str
   if (e == cudaSuccess) e = cudaMemsetAsync(tmp.d_work, 0, 256 + 256, sy->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(tmp.d_thr, thr.data(), nsteps * sizeof(BThr), cudaMemcpyHostToDevice, sy->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_rec, 0, (size_t)nsteps * 64 * sizeof(int64_t), sy->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(blk + o_wide, 0, kWideScratch, sy->stream);
   if (e != cudaSuccess) {
     release();
     return cuda_fail(e, "resident_run set-up");
@@ -2204,8 +2353,24 @@ int resident_run(sa_system* sy, const double* T, int nsteps, int sweeps, int str
   sa_batch::Group& g = tmp.groups[0];
   g.stream = sy->stream;
   int mc = 0;
-  int status = dispatch(&tmp, g, 0, 0, 2, &mc);
-  if (status == SA_OK) {
+  int status = SA_OK;
+  if (g.wide) {
+    tmp.d_wide = blk + o_wide;
+    tmp.wide_cap = 1;
+    tmp.run_start.assign(1, 0);
+    status = launch_wide(&tmp, g, d.sweep_limit, d_rec);
+    tmp.d_wide = nullptr;  // part of blk
+    if (status == SA_OK) {
+      e = cudaMemcpyAsync(&st, tmp.d_state, sizeof st, cudaMemcpyDeviceToHost, sy->stream);
+      if (e == cudaSuccess && step_E)
+        e = cudaMemcpyAsync(step_E, d_rec, (size_t)nsteps * 64 * sizeof(int64_t), cudaMemcpyDeviceToHost, sy->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(sy->stream);
+      if (e != cudaSuccess) status = cuda_fail(e, "resident_run");
+    }
+  } else {
+    status = dispatch(&tmp, g, 0, 0, 2, &mc);
+  }
+  if (status == SA_OK && !g.wide) {
     BatchParams prm;
     batch_params(&tmp, d.sweep_limit, &prm);
     prm.order = tmp.d_order;

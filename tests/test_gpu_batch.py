@@ -286,3 +286,64 @@ def test_fused_single_slot_measurement_full_batch(sab, stride):
         assert done == nsteps * per
         assert np.array_equal(E.astype(np.float32), mn), i
         assert np.array_equal(b.spins(i, 0), o.spins()), i
+
+
+@pytest.mark.parametrize("L,stride", [(40, 1), (42, 3), (64, 1)])
+def test_wide_single_slot_anneal(sab, L, stride):
+    """A lone single-slot 3D anneal of L >= 40 runs wide (every column of a
+    colour a lane group anywhere on the GPU, three launches per sweep); its
+    running maxima and spins match annealing<> and the resident form."""
+    from simulated_annealing_b200.batch import KERNEL_AUTO, KERNEL_NO_WIDE, Batch
+    nsteps, per = 3, 3
+    T0, T1 = 2.8, 0.4
+    Ts = [T0 + (T1 - T0) * k / (nsteps - 1) for k in range(nsteps)]
+    o = O.OracleSystem(O.LAT_3D, L, mode=O.MODE_PHILOX)
+    o.set_seed(77)
+    o.init_J()
+    o.set_seed(78)
+    o.init_rand()
+    mn, _ = o.anneal(T0, 1, T1, nsteps, per, stride)
+    for kernel in (KERNEL_AUTO, KERNEL_NO_WIDE):
+        b = Batch(kernel)
+        b.set_measure_stride(stride)
+        sch = b.add_schedule(Ts, per)
+        b.add_instance(O.LAT_3D, L, schedule=sch, seed_J=77, seed=78)
+        b.finalize()
+        b.run(4)  # ends inside a step
+        b.run(100)  # stops at the end of the schedule
+        b.sync()
+        E, done = b.anneal_result(0)
+        assert done == nsteps * per
+        assert np.array_equal(E.astype(np.float32), mn), kernel
+        assert np.array_equal(b.spins(0, 0), o.spins()), kernel
+        b.close()
+
+
+def test_wide_anneal_in_a_full_batch(sab):
+    """Single-slot 3D anneals of L >= 48 run wide even beside many other
+    instances; every instance still matches annealing<>."""
+    from simulated_annealing_b200.batch import Batch
+    nsteps, per = 2, 3
+    T0, T1 = 2.5, 0.5
+    Ts = [T0 + (T1 - T0) * k / (nsteps - 1) for k in range(nsteps)]
+    b = Batch()
+    sch = b.add_schedule(Ts, per)
+    specs = [(O.LAT_3D, 48, 500)] + [(O.LAT_3D, 8, 501 + k) for k in range(300)]
+    for lat, L, s in specs:
+        b.add_instance(lat, L, schedule=sch, seed_J=s, seed=s + 1)
+    b.finalize()
+    b.run(5)
+    b.run(100)
+    b.sync()
+    for i in (0, 1, 299):
+        lat, L, s = specs[i]
+        o = O.OracleSystem(lat, L, mode=O.MODE_PHILOX)
+        o.set_seed(s)
+        o.init_J()
+        o.set_seed(s + 1)
+        o.init_rand()
+        mn, _ = o.anneal(T0, 1, T1, nsteps, per, 1)
+        E, done = b.anneal_result(i)
+        assert done == nsteps * per
+        assert np.array_equal(E.astype(np.float32), mn), i
+        assert np.array_equal(b.spins(i, 0), o.spins()), i

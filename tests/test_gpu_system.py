@@ -73,6 +73,19 @@ def test_long_sweeps_resident_path(sab, lat, L):
     _check(g, o)
 
 
+@pytest.mark.parametrize("L", [40, 48])
+def test_long_sweeps_wide_path(sab, L):
+    """Zero-field runs of >= 16 sweeps of a 3D lattice of L >= 40 go through
+    the wide form (the lattice over the whole GPU, three launches per sweep)."""
+    g, o = _pair(sab, O.LAT_3D, L, 0.7)
+    _setup((g, o), 11, 12)
+    for n in (20, 2, 17):
+        g.sweep(n)
+        o.sweep(n)
+        _check(g, o)
+    assert g.rng_state()[1] == o.draw
+
+
 def test_init_J_without_reset_consumes_draws(sab):
     # timing-mode flow (src/main_gpu.cu:165-166): init_J then sweeps continue at draw t
     g, o = _pair(sab, O.LAT_3D, 6, 0.8)
