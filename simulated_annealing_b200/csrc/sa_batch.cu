@@ -853,8 +853,9 @@ struct sa_batch {
   }
 };
 
-// Per wide group: 64 bond counters, the ticket, the end sweep.
+// Per wide group: its control block (WideCtl).
 constexpr size_t kWideScratch = 512;
+static_assert(sizeof(WideCtl) <= kWideScratch, "wide control block");
 // Sweeps per CUDA graph of the wide form (three kernel nodes each); a run
 // replays it and launches the remainder directly.
 constexpr int kWideGraphSweeps = 25;
@@ -1086,20 +1087,23 @@ static int launch_wide(sa_batch* b, const sa_batch::Group& g, long nsweeps, int6
   int64_t end = start + nsweeps;
   if (d.sweep_limit >= 0) end = std::min<int64_t>(end, d.sweep_limit);
   if (end <= start) return SA_OK;
-  char* scratch = b->d_wide + (size_t)g.wide_slot * kWideScratch;
   WideParams wp;
-  wp.inst = b->d_inst;
-  wp.state = b->d_state;
-  wp.id = id;
-  wp.mstride = b->mstride;
-  wp.spins = b->d_spins;
-  wp.J = b->d_J;
-  wp.thr = b->d_thr;
+  memset(&wp, 0, sizeof wp);  // compared bytewise by the graph cache
+  wp.st = b->d_state + d.state_idx;
+  wp.ctl = reinterpret_cast<WideCtl*>(b->d_wide + (size_t)g.wide_slot * kWideScratch);
+  wp.S = b->d_spins + d.spin_off;
+  wp.J = b->d_J + d.J_off;
+  wp.thr = b->d_thr + d.thr_off;
   wp.step_rec = step_rec;
-  wp.cnt = reinterpret_cast<unsigned*>(scratch);
-  wp.ticket = reinterpret_cast<unsigned*>(scratch + 256);
-  int64_t* d_end = reinterpret_cast<int64_t*>(scratch + 264);
-  wp.end = d_end;
+  wp.half = d.half;
+  wp.N = d.N;
+  wp.nbonds = d.nbonds;
+  wp.state_idx = d.state_idx;
+  wp.seed = d.seed;
+  wp.L = d.L;
+  wp.sweeps_per_step = d.sweeps_per_step;
+  wp.thr_count = d.thr_count;
+  wp.mstride = b->mstride;
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
   const long threads = (long)d.L * (d.L / 2) * wide_lanes(d.L);
@@ -1108,7 +1112,7 @@ static int launch_wide(sa_batch* b, const sa_batch::Group& g, long nsweeps, int6
   // threads that none counts more than 10 sites (its bond count stays below 32)
   const long egrid = std::max<long>(std::min<long>((d.N + kWideThreads - 1) / kWideThreads, (long)sms),
                                     (d.N + 10L * kWideThreads - 1) / (10L * kWideThreads));
-  k_wide_set_end<<<1, 1, 0, g.stream>>>(d_end, end);
+  k_wide_begin<<<1, 32, 0, g.stream>>>(wp, end);
   SA_CUDA_TRY(cudaGetLastError());
   auto sweeps = [&](int64_t n) {
     for (int64_t i = 0; i < n; ++i) {

@@ -21,18 +21,33 @@
 
 namespace sa {
 
+// Control block of one wide instance (device memory, one per wide group):
+// the counters of the sweep being measured and a mirror of the instance's
+// progress that every launch reads in one cache line.
+struct WideCtl {
+  unsigned cnt[64];   // satisfied bonds of the sweep being measured (zero between sweeps)
+  unsigned ticket;    // blocks of the end-of-sweep launch done (zero between sweeps)
+  unsigned pad;
+  int64_t end;        // sweeps stop at this count (the run's, or the schedule's, end)
+  int64_t sweeps;     // sweeps done (mirror of the instance state)
+  uint64_t draw;      // next draw index (mirror)
+  uint32_t th[8];     // acceptance thresholds of the current step
+};
+
+// Everything a wide launch needs, by value: the instance's geometry and
+// buffers come from the host, so no launch starts with a chain of dependent
+// loads (descriptor, state, thresholds) before its real work.
 struct WideParams {
-  const InstDesc* inst;
-  InstState* state;
-  int32_t id;          // the instance's index in inst
-  int32_t mstride;     // measure every mstride sweeps of a step (0 = never)
-  word_t* spins;
-  const word_t* J;
-  const BThr* thr;
-  int64_t* step_rec;   // last measured -H at the end of every step, [state][step][64], or null
-  unsigned* cnt;       // [64] satisfied bonds of the sweep being measured (zero between sweeps)
-  unsigned* ticket;    // blocks of the end-of-sweep launch done (zero between sweeps)
-  const int64_t* end;  // sweeps stop at this count (the run's, or the schedule's, end)
+  InstState* st;
+  WideCtl* ctl;
+  word_t* S;            // the instance's spins, [colour][row][k]
+  const word_t* J;      // its couplings, [axis][colour][row][k]
+  const BThr* thr;      // its schedule's thresholds, one per step
+  int64_t* step_rec;    // last measured -H at the end of every step, [state][step][64], or null
+  int64_t half, N, nbonds, state_idx;
+  uint64_t seed;
+  int32_t L, sweeps_per_step, thr_count;
+  int32_t mstride;      // measure every mstride sweeps of a step (0 = never)
 };
 
 constexpr int kWideThreads = 256;
@@ -46,11 +61,10 @@ __host__ __device__ constexpr int wide_lanes(int L) {
 // Half-sweep of colour c. Thread t serves column t / G (row-major (y, k) over
 // the L x L/2 columns of the colour), segment t % G of its planes.
 __global__ void __launch_bounds__(kWideThreads) k_wide_half(WideParams p, int c) {
-  const InstDesc d = p.inst[p.id];
-  const InstState* st = p.state + d.state_idx;
-  const int64_t sweeps = st->sweeps;  // written only by the end-of-sweep launch
-  if (sweeps >= *p.end) return;       // the same for the whole grid
-  const int L = d.L, hL = L >> 1;
+  const WideCtl* ctl = p.ctl;
+  const int64_t sweeps = ctl->sweeps;  // written only by the end-of-sweep launch
+  if (sweeps >= ctl->end) return;      // the same for the whole grid
+  const int L = p.L, hL = L >> 1;
   const int G = wide_lanes(L);
   const int lane = threadIdx.x & 31;
   const long gt = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -66,26 +80,22 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_half(WideParams p, int c)
   x_neighbours(k, par, hL, kw, ke);
   const int yn = (y == 0) ? L - 1 : y - 1, ys = (y == L - 1) ? 0 : y + 1;
   const long zg = (long)L * hL;  // z stride of spins and couplings
-  word_t* own = p.spins + d.spin_off + (long)c * d.half + (long)y * hL + k;
-  const word_t* so = p.spins + d.spin_off + (long)(1 - c) * d.half;
+  word_t* own = p.S + (long)c * p.half + (long)y * hL + k;
+  const word_t* so = p.S + (long)(1 - c) * p.half;
   const word_t* pw = so + (long)y * hL + kw;
   const word_t* pe = so + (long)y * hL + ke;
   const word_t* pn = so + (long)yn * hL + k;
   const word_t* ps = so + (long)ys * hL + k;
-  const word_t* Jb = p.J + d.J_off;
-  const word_t* Jxc = Jb + (long)(0 + c) * d.half;
-  const word_t* Jxo = Jb + (long)(1 - c) * d.half;
-  const word_t* Jyc = Jb + (long)(2 + c) * d.half;
-  const word_t* Jyo = Jb + (long)(3 - c) * d.half;
-  const word_t* Jzc = Jb + (long)(4 + c) * d.half;
+  const word_t* Jxc = p.J + (long)(0 + c) * p.half;
+  const word_t* Jxo = p.J + (long)(1 - c) * p.half;
+  const word_t* Jyc = p.J + (long)(2 + c) * p.half;
+  const word_t* Jyo = p.J + (long)(3 - c) * p.half;
+  const word_t* Jzc = p.J + (long)(4 + c) * p.half;
   const long jo = (long)y * hL + k, je = (long)y * hL + ke, js = (long)ys * hL + k;
-  int64_t s = sweeps / d.sweeps_per_step;
-  if (s > d.thr_count - 1) s = d.thr_count - 1;
   uint32_t th[8];
-  const BThr* tp = p.thr + d.thr_off + s;
 #pragma unroll
-  for (int q = 0; q < 8; ++q) th[q] = tp->dn[q];
-  const uint64_t draw = st->draw + c;
+  for (int q = 0; q < 8; ++q) th[q] = ctl->th[q];
+  const uint64_t draw = ctl->draw + c;
   const unsigned long long site0 = (unsigned long long)(xx + L * y), plane = (unsigned long long)L * L;
   // segment g: planes [z0, z0 + ls), sizes as even as L allows (ls >= 2)
   const int sbase = L / G, srem = L % G;
@@ -102,7 +112,7 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_half(WideParams p, int c)
     const word_t jw = __ldg(Jxc + jo + zo), jee = __ldg(Jxo + je + zo);
     const word_t jn = __ldg(Jyc + jo + zo), jss = __ldg(Jyo + js + zo);
     const word_t ju = __ldg(Jzc + jo + zo), jd = __ldg(Jzc + jo + (long)zn * zg);
-    const uint32_t u = philox_draw(d.seed, site0 + plane * (unsigned)z, draw);
+    const uint32_t u = philox_draw(p.seed, site0 + plane * (unsigned)z, draw);
     word_t c0, c1, c2;
     count5(jw ^ sw ^ si, jee ^ se ^ si, jn ^ sn ^ si, jss ^ ss ^ si, jd ^ sd ^ si, c0, c1, c2);
     uint32_t m0, m1, m2;
@@ -167,25 +177,24 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_half(WideParams p, int c)
 
 // End of a sweep. A measured sweep's -H: every block counts the satisfied
 // bonds of its sites (each bond once, from its site towards -x/-y/-z) and
-// adds them to cnt; the last block to finish (ticket) folds the totals into
-// the anneal record. That block then advances the sweep counter and the draw
-// index for the next sweep's launches.
+// adds them to the control block; the last block to finish (ticket) folds the
+// totals into the anneal record. That block then advances the sweep counter,
+// the draw index and the step's thresholds for the next sweep's launches.
 __global__ void __launch_bounds__(kWideThreads) k_wide_end(WideParams p) {
   __shared__ unsigned s_cnt[64];
   __shared__ int s_last;
-  const InstDesc d = p.inst[p.id];
-  InstState* st = p.state + d.state_idx;
-  const int64_t sweeps = st->sweeps;
-  if (sweeps >= *p.end) return;  // the same for the whole grid: no ticket is taken
-  const bool meas = p.mstride > 0 && (sweeps % d.sweeps_per_step) % p.mstride == 0;
+  WideCtl* ctl = p.ctl;
+  const int64_t sweeps = ctl->sweeps;
+  if (sweeps >= ctl->end) return;  // the same for the whole grid: no ticket is taken
+  const bool meas = p.mstride > 0 && (sweeps % p.sweeps_per_step) % p.mstride == 0;
   const int lane = threadIdx.x & 31;
   if (threadIdx.x < 64) s_cnt[threadIdx.x] = 0;
   __syncthreads();
   if (meas) {
-    const int L = d.L, hL = L >> 1;
-    const long half = d.half, plane = (long)L * hL;
-    const word_t* S = p.spins + d.spin_off;
-    const word_t* J = p.J + d.J_off;
+    const int L = p.L, hL = L >> 1;
+    const long half = p.half, plane = (long)L * hL;
+    const word_t* S = p.S;
+    const word_t* J = p.J;
     VCount<4> sm;
     VCount<16> big;
     sm.clear();
@@ -194,7 +203,8 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_end(WideParams p) {
     // a thread's count stays below 32 (at most 10 sites of 3 bonds: the host
     // sizes the grid for it), so five planes carry it and the warp sum widens
     // by one plane per level
-    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < d.N; t += (long)gridDim.x * blockDim.x) {
+#pragma unroll 2
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < p.N; t += (long)gridDim.x * blockDim.x) {
       const int c = t >= half ? 1 : 0;
       const long rem = t - (long)c * half;
       const long r = rem / hL;
@@ -212,7 +222,7 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_end(WideParams p) {
       const word_t u = __ldg(J + (long)(4 + c) * half + rem) ^ si ^ Sc[(long)wrap_dec(z, L) * plane + (long)y * hL + k];
       add2_small(sm, w ^ n ^ u, (w & n) | (u & (w ^ n)));
       if (++it == 5) {  // <= 3 per site: the 4-plane counter stays below 16
-        add_small(big, sm);
+        add_small_w<5>(big, sm);
         sm.clear();
         it = 0;
       }
@@ -222,39 +232,59 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_end(WideParams p) {
     atomicAdd(&s_cnt[lane], big.count_of(lane));
     atomicAdd(&s_cnt[lane + 32], big.count_of(lane + 32));
     __syncthreads();
-    if (threadIdx.x < 64 && s_cnt[threadIdx.x]) atomicAdd(p.cnt + threadIdx.x, s_cnt[threadIdx.x]);
+    if (threadIdx.x < 64 && s_cnt[threadIdx.x]) atomicAdd(ctl->cnt + threadIdx.x, s_cnt[threadIdx.x]);
   }
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(p.ticket, 1u) == gridDim.x - 1) ? 1 : 0;
+  if (threadIdx.x == 0) s_last = (atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1) ? 1 : 0;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
+  InstState* st = p.st;
+  const int64_t s1 = sweeps + 1;
   if (threadIdx.x < 64) {
     const int j = threadIdx.x;
     int64_t elast = st->elast[j];
     if (meas) {
-      const int64_t e = 2 * (int64_t)atomicExch(p.cnt + j, 0u) - d.nbonds;
+      const int64_t e = 2 * (int64_t)atomicExch(ctl->cnt + j, 0u) - p.nbonds;
       elast = e;
       st->elast[j] = e;
       st->emax[j] = (st->measured == 0) ? e : max(st->emax[j], e);
     }
-    const int64_t s1 = sweeps + 1;
-    if (p.step_rec && s1 % d.sweeps_per_step == 0) {
-      const int64_t stp = s1 / d.sweeps_per_step - 1;
-      if (stp < d.thr_count) p.step_rec[((int64_t)d.state_idx * d.thr_count + stp) * 64 + j] = elast;
+    if (p.step_rec && s1 % p.sweeps_per_step == 0) {
+      const int64_t stp = s1 / p.sweeps_per_step - 1;
+      if (stp < p.thr_count) p.step_rec[(p.state_idx * p.thr_count + stp) * 64 + j] = elast;
     }
+  }
+  if (threadIdx.x >= 64 && threadIdx.x < 72) {
+    int64_t sn = s1 / p.sweeps_per_step;
+    if (sn > p.thr_count - 1) sn = p.thr_count - 1;
+    ctl->th[threadIdx.x - 64] = p.thr[sn].dn[threadIdx.x - 64];
   }
   __syncthreads();  // st->measured has been read
   if (threadIdx.x == 0) {
     if (meas) st->measured += 1;
-    st->sweeps = sweeps + 1;
+    st->sweeps = s1;
     st->draw += 2;
-    *p.ticket = 0;
+    ctl->sweeps = s1;
+    ctl->draw += 2;
+    ctl->ticket = 0;
   }
 }
 
-// Sets the sweep count at which the wide launches of a run stop.
-__global__ void k_wide_set_end(int64_t* end, int64_t v) { *end = v; }
+// Starts a run: the control block takes the instance's progress, the step's
+// thresholds and the sweep count at which the run stops.
+__global__ void k_wide_begin(WideParams p, int64_t end) {
+  WideCtl* ctl = p.ctl;
+  const int64_t sweeps = p.st->sweeps;
+  int64_t s = sweeps / p.sweeps_per_step;
+  if (s > p.thr_count - 1) s = p.thr_count - 1;
+  if (threadIdx.x < 8) ctl->th[threadIdx.x] = p.thr[s].dn[threadIdx.x];
+  if (threadIdx.x == 0) {
+    ctl->end = end;
+    ctl->sweeps = sweeps;
+    ctl->draw = p.st->draw;
+  }
+}
 
 }  // namespace sa
