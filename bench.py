@@ -493,7 +493,7 @@ def run_single(args):
         s.sync()
         dt = time.perf_counter() - t0
         att = 10_000 * 4096 * 64 * args.steps
-        wl = "2D L=64 periodic, T=1.0, 10,000 sweeps per step (one launch per half-sweep)"
+        wl = "2D L=64 periodic, T=1.0, 10,000 sweeps per step (one resident-kernel launch per step)"
     elif args.workload == "c2":
         s = GpuSystem("3d", 32, 3.0)
         s.set_seed(3); s.init_J(); s.set_seed(3); s.init_rand()
