@@ -61,7 +61,7 @@ int sa_batch_histogram(sa_batch_t b, int instance, int slot, int32_t* out, long 
 /* Kernel choice, before finalize: 0 (default) keeps every instance whose
  * spins fit in the shared memory of a cluster of <= 16 CTAs resident there for
  * a whole launch and runs the rest in the global-memory kernel, except that a
- * single-slot 3D anneal of L >= 32 with the GPU nearly to itself runs wide
+ * single-slot 3D anneal of L >= 40 with the GPU nearly to itself runs wide
  * (every column of a colour a lane group anywhere on the GPU, three launches
  * per sweep); 1 runs every instance in the global-memory kernel; 2 is 0
  * without the wide form. */

@@ -70,7 +70,7 @@ KERNEL_AUTO, KERNEL_GLOBAL, KERNEL_NO_WIDE = 0, 1, 2
 
 class Batch:
     """kernel: KERNEL_AUTO keeps instances resident in cluster shared memory
-    where they fit (a lone single-slot 3D anneal of L >= 32 runs wide, over
+    where they fit (a lone single-slot 3D anneal of L >= 40 runs wide, over
     the whole GPU); KERNEL_GLOBAL streams every instance from global memory;
     KERNEL_NO_WIDE is KERNEL_AUTO without the wide form."""
 

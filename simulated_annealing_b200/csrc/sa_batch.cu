@@ -859,13 +859,13 @@ static_assert(sizeof(WideCtl) <= kWideScratch, "wide control block");
 // Sweeps per CUDA graph of the wide form (three kernel nodes each); a run
 // replays it and launches the remainder directly.
 constexpr int kWideGraphSweeps = 25;
-// 3D L from which a single-slot anneal runs wide: always from kWideMinL (its
-// resident walk is latency-bound even in a full batch: L=48 50.7 -> 29 us per
-// sweep, L=64 98.9 -> 35.7), and from kWideSpreadL when the batch is spread
-// (below it the segmented resident walk on one cluster is faster: L=32 15.3
-// against 22.1 us per sweep).
-constexpr int kWideMinL = 48;
-constexpr int kWideSpreadL = 40;
+// 3D L from which a single-slot anneal runs wide when the batch leaves SMs
+// idle (spread). Alone, per sweep: L=40 34.3 -> 20.6 us, L=48 50.8 -> 23.5,
+// L=64 98.7 -> 29.8; L=32 stays on its cluster (15.4 against 22.1 wide). In a
+// full batch the resident form stays: the wide launches are latency-bound and
+// take SM time from the rest (a backlog-bound stream of 2,000 serving
+// requests fell from 1426 to 1233 attempts/ns with them).
+constexpr int kWideMinL = 40;
 
 // Shared-memory budget of one CTA of the resident kernel: the 227 KB opt-in
 // limit minus room for its static arrays (counters, per-warp planes).
@@ -986,10 +986,10 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
     // chained walk is latency-bound; beyond that it is throughput-bound and the
     // segments' extra map and scan work costs more than it saves (measured:
     // 3D L=32 on 16 CTAs 49.8 -> 17.2 us per sweep, L=64 97.6 -> 136.7).
-    // A lone single-slot 3D anneal of L >= kWideMinL leaves even a 16-CTA
-    // cluster latency-bound; it runs wide, over the whole GPU.
-    const bool wide = C != 0 && d.lattice == SA_LATTICE_3D && d.nslots == 1 && d.sched >= 0 && !b->no_wide &&
-                      (d.L >= kWideMinL || (b->spread && d.L >= kWideSpreadL));
+    // A single-slot 3D anneal of L >= kWideMinL with the GPU nearly to itself
+    // leaves even a 16-CTA cluster latency-bound; it runs wide, over the GPU.
+    const bool wide = C != 0 && b->spread && d.lattice == SA_LATTICE_3D && d.nslots == 1 && d.sched >= 0 &&
+                      !b->no_wide && d.L >= kWideMinL;
     bool seg = C != 0 && b->spread && d.lattice == SA_LATTICE_3D && d.nslots == 1 && d.L > 4 && !wide;
     if (seg) {
       const long lanes = (long)((d.L + C - 1) / C) * (d.L / 2) * seg_lanes(d.L);

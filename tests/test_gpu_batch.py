@@ -319,9 +319,10 @@ def test_wide_single_slot_anneal(sab, L, stride):
         b.close()
 
 
-def test_wide_anneal_in_a_full_batch(sab):
-    """Single-slot 3D anneals of L >= 48 run wide even beside many other
-    instances; every instance still matches annealing<>."""
+def test_large_anneal_in_a_full_batch(sab):
+    """A large single-slot 3D anneal beside many other instances stays on its
+    cluster (the wide form is for a GPU with idle SMs); every instance still
+    matches annealing<>."""
     from simulated_annealing_b200.batch import Batch
     nsteps, per = 2, 3
     T0, T1 = 2.5, 0.5
