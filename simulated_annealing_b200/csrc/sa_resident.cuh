@@ -17,6 +17,8 @@
 #pragma once
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include "sa_batch.hpp"
 #include "sa_device.cuh"
 
@@ -323,6 +325,10 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
     if (valid) prev = ldw<SL>(x.sm + own + (L - 1) * zs);
     SlotWords<SL> first = {};
     word_t jnext = __ldg(Jzc + jo);  // the z-1 coupling of the next plane (plane 0: the wrapped bond)
+    // A warp whose lanes all have a site and a slot (every warp of the
+    // batched ensembles) walks without the per-lane test.
+    auto walk = [&](auto check) {
+    constexpr bool CHECK = decltype(check)::value;
     for (int z0 = 0; z0 < L; z0 += P) {
       // Lane (column cl, i) draws the Philox number and loads the coupling
       // words of plane z0+i; the column's P lanes share them by shuffles, so
@@ -355,7 +361,7 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         const word_t ju = jnext;
         const word_t jd = (P == 1) ? bd : __shfl_sync(0xffffffffu, bd, src);
         jnext = jd;
-        if (valid) {
+        if (!CHECK || valid) {
           const bool last = (z == L - 1);
           const SlotWords<SL> si = ldw<SL>(x.sm + own);
           const SlotWords<SL> sd = last ? first : ldw<SL>(x.sm + own + zs);
@@ -384,6 +390,9 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         ps.step(zss);
       }
     }
+    };
+    if (__all_sync(0xffffffffu, valid)) walk(std::false_type{});
+    else walk(std::true_type{});
   }
 }
 
