@@ -232,6 +232,12 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
         sadr = (uint32_t)(ps.p - x.sm) + (uint32_t)(k * ns);
       }
     }
+    // A warp whose 32 sites all exist and whose lanes all have a slot (every
+    // warp but the last of the batched ensembles) updates without the
+    // per-lane test.
+    const bool all_upd = base + 32 <= tot && __all_sync(0xffffffffu, slot_ok);
+    auto subs = [&](auto check) {
+    constexpr bool CHECK = decltype(check)::value;
 #pragma unroll 1
     for (int sub = 0; sub < P; ++sub) {
       const int sl = sub * SPS + lane / P;
@@ -243,7 +249,7 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
       const uint32_t f = share(pk), na = share(nadr), sa = share(sadr);
       const int t = base + sl;
       const bool upd = t < tot && slot_ok;
-      if (BF || upd) {
+      if (!CHECK || BF || upd) {
         const int sk = slot ^ (int)(f & 0xFFu);
         const int own = rc + sk;
         const SlotWords<SL> si = ldw<SL>(x.sm + own);
@@ -277,9 +283,12 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
           prefix_bits(u, border ? tb[q] : th[q], m0, m1, m2);
           out.w[q] = flip_below(si.w[q], c0, c1, c2, m0, m1, m2);
         }
-        if (!BF || upd) stw<SL>(x.sm + own, out);
+        if (!CHECK || !BF || upd) stw<SL>(x.sm + own, out);
       }
     }
+    };
+    if (all_upd) subs(std::false_type{});
+    else subs(std::true_type{});
   }
 }
 
