@@ -822,9 +822,10 @@ __device__ __forceinline__ void rmeasure_body(const ResCtx& x, bool d3, bool ope
     wopen = open && xx == 0;
   };
   // satisfied-bond bits (q1 q0 = 0..3) of this lane's site in plane z
+  // lanes past the last column read column 0 (in range) and count nothing:
+  // the unit has no divergent branch
   auto unit_bits = [&](word_t& q0, word_t& q1) {
-    q0 = q1 = 0;
-    if (!ok) return;
+    const word_t okm = ok ? ~0ULL : 0ULL;
     const word_t* jp = Jc + (jr0 + z * zg);
     const word_t si = x.sm[own0 + z * zs];
     const word_t w = wopen ? 0 : (__ldg(jp) ^ si ^ x.sm[w0 + z * zs]);
@@ -832,11 +833,11 @@ __device__ __forceinline__ void rmeasure_body(const ResCtx& x, bool d3, bool ope
     if (d3) {
       const int zu = (z == 0) ? L - 1 : z - 1;
       const word_t uu = __ldg(jp + 4 * x.half) ^ si ^ x.sm[own0 + zu * zs];
-      q0 = w ^ n ^ uu;
-      q1 = (w & n) | (uu & (w ^ n));
+      q0 = (w ^ n ^ uu) & okm;
+      q1 = ((w & n) | (uu & (w ^ n))) & okm;
     } else {
-      q0 = w ^ n;
-      q1 = w & n;
+      q0 = (w ^ n) & okm;
+      q1 = (w & n) & okm;
     }
   };
   auto advance = [&]() {
