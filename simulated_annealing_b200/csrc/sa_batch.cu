@@ -859,6 +859,8 @@ static_assert(sizeof(WideCtl) <= kWideScratch, "wide control block");
 // Sweeps per CUDA graph of the wide form (three kernel nodes each); a run
 // replays it and launches the remainder directly.
 constexpr int kWideGraphSweeps = 25;
+// Wide-form graphs a batch keeps (one per distinct launch parameters).
+constexpr size_t kWideGraphCache = 32;
 // 3D L from which a single-slot anneal runs wide when the batch leaves SMs
 // idle (spread). Alone, per sweep: L=40 34.3 -> 20.6 us, L=48 50.8 -> 23.5,
 // L=64 98.7 -> 29.8; L=32 stays on its cluster (15.4 against 22.1 wide). In a
@@ -1128,6 +1130,13 @@ static int launch_wide(sa_batch* b, const sa_batch::Group& g, long nsweeps, int6
     cudaGraphExec_t exec = nullptr;
     for (const auto& w : b->wide_graphs)
       if (w.hgrid == hgrid && w.egrid == (unsigned)egrid && memcmp(&w.wp, &wp, sizeof wp) == 0) exec = w.exec;
+    if (!exec && b->wide_graphs.size() >= kWideGraphCache) {
+      // a server's requests come and go, each with its own parameters: keep
+      // the cache bounded (destroyed once no replay can be in flight)
+      SA_CUDA_TRY(cudaDeviceSynchronize());
+      for (auto& w : b->wide_graphs) cudaGraphExecDestroy(w.exec);
+      b->wide_graphs.clear();
+    }
     if (!exec) {
       cudaGraph_t graph = nullptr;
       if (cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeRelaxed) == cudaSuccess) {

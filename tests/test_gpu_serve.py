@@ -130,3 +130,23 @@ def test_serve_rejects_bad_requests(sab):
     with pytest.raises(SAError):
         srv.submit("2d", 8, 1, 2, [1.0], 0)
     assert srv.submit("3d", 64, 1, 2, [1.0], 1) is None  # 4 MiB of words > the pool
+
+
+def test_serve_many_wide_requests(sab):
+    """Large 3D requests served one at a time each run wide (alone on the
+    GPU) with their own captured graphs; more of them than the graph cache
+    holds still give annealing<>'s results."""
+    from simulated_annealing_b200.serve import Server
+    srv = Server(budget_bytes=64 << 20, max_requests=4)
+    T = linear(2.5, 0.5, 3)
+    out = {}
+    ids = []
+    for k in range(36):
+        rid = srv.submit(O.LAT_3D, 40, 900 + k, 950 + k, T, 20)
+        assert rid is not None
+        ids.append(rid)
+        drain(srv, 100, out)
+    for k in (0, 17, 35):
+        mn, spins = oracle_result(O.LAT_3D, 40, 900 + k, 950 + k, 2.5, 0.5, 3, 20)
+        assert np.array_equal(out[ids[k]].emax.astype(np.float32), mn), k
+        assert np.array_equal(out[ids[k]].spins, spins), k
