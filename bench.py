@@ -21,13 +21,19 @@ roofline   algorithmic bytes per launch (per site and slot and sweep: spins read
            bandwidth.
 cpu_baseline / --impl reference: the reference's own CPU classes (cpu_2d,
            cpu_3d, parallel_tempering<>) compiled from its sources, on a bounded
-           sample of the same instances, timed on this host.
-plain      the plain one-instance-per-launch form on the same GPU
-           (simulated_annealing_b200/sa_plain_pt: one system per slot, one launch
-           per half-sweep, a measurement copy per slot per sweep and a host
-           exchange per sweep, as parallel_tempering<gpu_sys> drives gpu_3d) on
-           a bounded sample of the same instances; batched_over_plain = value /
-           its rate.
+           sample of the same instances, timed on this host: one instance per
+           host thread (the template's OpenMP loop over slots set to 1 thread),
+           as many threads as cores.
+plain      the plain one-instance-per-launch form on the same GPU: each
+           instance of a bounded sample alone in its own batch (the engine's
+           resident kernel, one launch of --sweeps-per-step sweeps with an
+           exchange per sweep), launched back to back on one stream;
+           batched_over_plain = value / its rate.
+plain_host_driven  the reference's own driving pattern on the same GPU
+           (simulated_annealing_b200/sa_plain_pt: one system per slot, one
+           launch per half-sweep, a measurement copy per slot per sweep and a
+           host exchange per sweep, as parallel_tempering<gpu_sys> drives
+           gpu_3d).
 serving    continuous batching of anneal requests (simulated_annealing_b200.serve):
            Poisson arrivals at 2,000/s, 2D L 16..128 or 3D L 8..64 with equal
            probability (L log-uniform, rounded to even), sweeps log-uniform in
@@ -38,6 +44,12 @@ serving    continuous batching of anneal requests (simulated_annealing_b200.serv
            the first half of them at --serve-sustainable-rate (30/s), a rate the
            GPU keeps up with; --workload serve runs the whole 20,000 (or
            --serve-requests) at --serve-rate.
+
+--gpus N   one process per GPU (torch.distributed over NCCL): when WORLD_SIZE is
+           unset the script launches its N ranks itself (torch.distributed.run
+           on 127.0.0.1); every rank runs its own block of the instance
+           sequence (weak scaling, no collective on the data path) and rank 0
+           prints the line with the max-over-ranks times.
 
 --workload c1|c2|c3 time the single-lattice cases instead (2D L=64 T=1.0 for
 10,000 sweeps; 3D L=32 anneal 3.0 -> 0.2 over 200 x 100 sweeps; 3D L=16
@@ -113,20 +125,19 @@ def measured_hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic():
-    """DRAM read+write bytes of one step of the resident kernel from the
-    committed ncu summary (profiles/k_resident_c4.md, line
-    'traffic_bytes_per_step: N'): the state is loaded into shared memory once
-    and stored once per launch, so the traffic does not grow with the sweeps
-    per step."""
-    p = os.path.join(ROOT, "profiles", "k_resident_c4.md")
-    try:
-        for line in open(p):
-            if line.strip().startswith("traffic_bytes_per_step:"):
-                return float(line.split(":", 1)[1].strip().split()[0])
-    except Exception:
-        pass
-    return None
+def launch_traffic_bytes(insts, nslots=16) -> int:
+    """DRAM bytes one launch of the resident kernel moves: every instance's
+    spins come from HBM into shared memory once and go back once, and its
+    couplings (compact: dim words per site) are read once; the sweeps in
+    between run out of shared memory and L2. An ncu capture of a small case
+    of the same kernel (dram__bytes_read.sum + dram__bytes_write.sum) agrees
+    with this count; it does not grow with the sweeps per launch."""
+    total = 0
+    for lat, L, _ in insts:
+        N = site_count(lat, L)
+        d = 3 if lat == 2 else 2
+        total += 2 * 8 * N * nslots + 8 * d * N
+    return total
 
 
 class ClockSampler:
@@ -186,29 +197,31 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- CPU
-def cpu_reference_sample(insts, budget_s: float, sweeps_per_instance: int = 50):
+def cpu_reference_sample(insts, budget_s: float, sweeps_per_instance: int = 50, threads: int = 0):
     """The reference's parallel_tempering<cpu_sys> over cpu_2d / cpu_3d systems
     (built as its driver builds them: set_seed; init_J; set_seed; init_rand), on
     the first instances of the workload until `budget_s` of CPU work is done.
-    Instances run concurrently in host threads, each template using OpenMP over
-    its 16 slots, so all host cores are busy."""
-    ncpu = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(min(16, ncpu)))
+    One instance per host thread, each thread's OpenMP loop over the slots set
+    to one thread, as many threads as cores (ctypes releases the GIL during
+    the reference's calls)."""
+    ncpu = threads or os.cpu_count() or 1
     from oracle import oracle as O
 
     if not O.ref_available():
         O.build()
-    omp = int(os.environ["OMP_NUM_THREADS"])
-    workers = max(1, ncpu // max(1, omp))
+    lib = O.ref_lib()
     lock = threading.Lock()
-    state = {"next": 0, "attempts": 0, "done": 0}
+    state = {"next": 0, "attempts": 0, "done": 0, "rate": 0.0}
     t0 = time.perf_counter()
     deadline = t0 + budget_s
 
     def work():
+        lib.ref_omp_threads(1)
+        att, busy = 0, 0.0
         while True:
             with lock:
                 if time.perf_counter() > deadline or state["next"] >= len(insts):
+                    state["rate"] += att / busy if busy > 0 else 0.0
                     return
                 k = state["next"]
                 state["next"] += 1
@@ -221,29 +234,38 @@ def cpu_reference_sample(insts, budget_s: float, sweeps_per_instance: int = 50):
                 s.set_seed(seed)
                 s.init_rand()
             pt = O.RefPT(systems, list(T), 1)
+            ts = time.perf_counter()
             for _ in range(sweeps_per_instance):
                 pt.step(0)
+            busy += time.perf_counter() - ts
+            a = sweeps_per_instance * len(T) * site_count(lat, L) * 64
+            att += a
             with lock:
-                state["attempts"] += sweeps_per_instance * len(T) * site_count(lat, L) * 64
+                state["attempts"] += a
                 state["done"] += 1
 
-    threads = [threading.Thread(target=work) for _ in range(workers)]
-    for th in threads:
+    threads_ = [threading.Thread(target=work) for _ in range(ncpu)]
+    for th in threads_:
         th.start()
-    for th in threads:
+    for th in threads_:
         th.join()
     dt = time.perf_counter() - t0
-    value = state["attempts"] / (dt * 1e9)
+    # every thread's attempts over its own stepping time (systems are built
+    # outside the timed loops), summed over the concurrently running threads
+    value = state["rate"] / 1e9
     sample = (f"{state['done']} instances of the mix x 16 slots x {sweeps_per_instance} sweeps "
-              f"(+ exchange each sweep), {workers} instance threads x OMP {omp}, {dt:.1f} s")
-    return {"value": value, "unit": UNIT, "cores": min(ncpu, workers * omp), "kind": "reference",
-            "sample": sample}
+              f"(+ exchange each sweep; the template measures every slot before it), {ncpu} instance "
+              f"threads x 1 OpenMP thread, {dt:.1f} s")
+    return {"value": value, "unit": UNIT, "cores": ncpu, "kind": "reference", "sample": sample,
+            "per_core": value / ncpu}
 
 
 # ----------------------------------------------------------------------------- plain form
-def plain_sample(insts, budget_s: float, sweeps: int = 20):
-    """The plain one-instance-per-launch PT form over the first instances of the
-    workload (sa_plain_pt), until `budget_s` of timed loops."""
+def plain_host_driven_sample(insts, budget_s: float, sweeps: int = 20):
+    """The reference's driving pattern over the first instances of the workload
+    (sa_plain_pt: one system per slot, one launch per half-sweep, a blocking
+    measurement per slot per sweep and a host exchange), until `budget_s` of
+    timed loops."""
     exe = os.path.join(ROOT, "simulated_annealing_b200", "sa_plain_pt")
     lines = []
     for lat, L, seed in insts:
@@ -258,6 +280,44 @@ def plain_sample(insts, budget_s: float, sweeps: int = 20):
     return {"value": att / sec / 1e9, "unit": UNIT,
             "sample": f"{done} instances of the mix x 16 slots x {sweeps} sweeps (+ exchange each sweep), "
                       f"{sec:.1f} s of timed loops"}
+
+
+def plain_per_instance_sample(insts, sweeps: int, stream, reps: int = 2):
+    """The plain one-instance-per-launch form: every instance of `insts` alone
+    in its own batch (the resident kernel, one launch of `sweeps` sweeps with
+    an exchange per sweep), the launches back to back on one stream; device
+    time (CUDA events) over `reps` rounds after one warm-up round."""
+    import torch
+
+    from simulated_annealing_b200.batch import Batch
+
+    batches = []
+    for lat, L, seed in insts:
+        b = Batch()
+        lad = b.add_ladder(LADDER_3D if lat == 2 else LADDER_2D)
+        b.add_instance(lat, L, ladder=lad, seed_J=seed, seed=seed)
+        b.finalize()
+        b.set_stream(stream.cuda_stream)
+        batches.append(b)
+    for b in batches:
+        b.run(sweeps)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        for b in batches:
+            b.run(sweeps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    att = reps * sweeps * 64 * sum(b.site_slots() for b in batches)
+    launches = reps * sum(b.launches_per_run() for b in batches)
+    for b in batches:
+        b.close()
+    return {"value": att / (ms * 1e6), "unit": UNIT,
+            "sample": f"first {len(insts)} instances of the mix, each alone in its own batch, x 16 slots x "
+                      f"{sweeps} sweeps (+ exchange each sweep), {reps} rounds of back-to-back launches "
+                      f"({launches} launches, {ms:.1f} ms device time)"}
 
 
 # ----------------------------------------------------------------------------- serving
@@ -303,37 +363,86 @@ def serving_run(n: int, rate: float, budget_gb: float, chunk: int = 100):
 
 
 # ----------------------------------------------------------------------------- GPU
-def run_ours(args):
-    import torch
+def c4_config(args, world: int) -> dict:
+    S = args.sweeps_per_step
+    return {"workload": f"batched PT mix: {args.instances} instances x 16 slots, 2D L{{16..64}} / "
+                        f"3D L{{8..24}}, {S} sweeps + exchange per sweep per step",
+            "instances_per_gpu": args.instances, "slots": 16, "sweeps_per_step": S,
+            "l2": "inputs larger than L2 (1.9 GB of spins)",
+            "parallelism": f"instances sharded, {world} GPU(s), no collective"}
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
 
-        import torch.distributed as dist_mod
-
-        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        dist = dist_mod
-
+def build_c4_batch(insts, stream_ptr=None):
+    """The batched mix as the bench runs it: one batch, the two 16-slot
+    ladders, the instances in order (tests build the same batch)."""
     from simulated_annealing_b200.batch import Batch
 
-    insts = shard_instances(rank, world, args.instances)
     b = Batch()
     l2 = b.add_ladder(LADDER_2D)
     l3 = b.add_ladder(LADDER_3D)
     for lat, L, seed in insts:
         b.add_instance(lat, L, ladder=(l3 if lat == 2 else l2), seed_J=seed, seed=seed)
     b.finalize()
+    if stream_ptr is not None:
+        b.set_stream(stream_ptr)
+    return b
+
+
+def init_ranks(backend: str):
+    """(world, rank, local_rank, dist module or None) from the torchrun
+    environment; the process group has a short timeout so that ranks waiting
+    for a dead peer end with an error."""
+    import datetime
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+    return world, rank, local, dist
+
+
+def run_stub(args):
+    """The multi-rank plumbing without a GPU (gloo): each rank takes its shard
+    of the instance sequence, reports a stand-in time that grows with its rank,
+    and rank 0 prints the line built from the max over ranks. Used by the CPU
+    tests of the launcher."""
+    world, rank, _, dist = init_ranks("gloo")
+    insts = shard_instances(rank, world, args.instances)
+    ms = 10.0 + rank
+    seeds = sum(s for _, _, s in insts)
+    ms, = max_over_ranks([ms], dist, "cpu")
+    tot = max_over_ranks([float(seeds)], None, "cpu")[0]
+    if dist:
+        import torch
+
+        t = torch.tensor([tot], dtype=torch.float64)
+        dist.all_reduce(t)
+        tot = float(t[0])
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "n_gpus": world, "ms_per_step": ms,
+                          "stub": True, "instances_total": world * args.instances, "seed_sum": tot}), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local, dist = init_ranks("nccl")
+    torch.cuda.set_device(local)
+
+    insts = shard_instances(rank, world, args.instances)
     stream = torch.cuda.Stream()
-    b.set_stream(stream.cuda_stream)
+    b = build_c4_batch(insts, stream.cuda_stream)
     S = args.sweeps_per_step
     site_slots = b.site_slots()
     attempts_step = site_slots * 64 * S
-    n_classes = b.launches_per_run()  # one launch per (lanes-per-site, cluster size) group
+    n_launch = b.launches_per_run()  # one launch per shape group
 
     def barrier():
         torch.cuda.synchronize()
@@ -386,35 +495,32 @@ def run_ours(args):
         bytes_launch = algorithmic_bytes_per_sweep(insts) * S
         launch_s = (ms / 1e3) / args.steps
         achieved = bytes_launch / launch_s / 1e9
-        traffic = profiled_traffic() if args.instances == 4096 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 (bitwise/int32)", "data": "synthetic",
-            "config": {"workload": "batched PT mix: 4096 instances x 16 slots, 2D L{16..64} / 3D L{8..24}, "
-                                   f"{S} sweeps + exchange per sweep per step",
-                       "instances_per_gpu": args.instances, "slots": 16, "sweeps_per_step": S,
-                       "site_slots_per_gpu": site_slots, "l2": "inputs larger than L2 (1.9 GB of spins)",
-                       "parallelism": f"instances sharded, {world} GPU(s), no collective"},
+            "config": dict(c4_config(args, world), site_slots_per_gpu=site_slots),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(np.mean(h2d)) if h2d else 0,
                     "d2h_bytes_per_step": int(E_host.numel() * 8 + 2 * npairs * 8)},
-            "gpu_launches": args.steps * n_classes,
+            "gpu_launches": args.steps * n_launch,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
+                         "frac": achieved / peak, "traffic": launch_traffic_bytes(insts),
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
                          else "fallback 6650 GB/s",
                          "algorithmic_bytes_per_launch": bytes_launch,
-                         "note": "state resident in shared memory for a launch: measured DRAM traffic per step "
-                                 "(traffic) is far below the algorithmic bytes; the kernel is integer-ALU issue "
-                                 "bound (profiles/k_resident_c4.md)"},
+                         "note": "state resident in shared memory for a launch: the DRAM traffic per launch "
+                                 "(spins in and out once, couplings once) is far below the algorithmic bytes; "
+                                 "the kernel is bound by integer-ALU issue"},
             "clocks": clk,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_sample(insts, args.cpu_budget)
-        if world == 1 and args.plain_budget > 0:
-            pl = plain_sample(insts, args.plain_budget)
+        if world == 1 and args.plain_instances > 0:
+            pl = plain_per_instance_sample(insts[:args.plain_instances], S, stream)
             line["plain"] = pl
             line["batched_over_plain"] = value / pl["value"]
+        if world == 1 and args.plain_budget > 0:
+            line["plain_host_driven"] = plain_host_driven_sample(insts, args.plain_budget)
         if world == 1 and args.serve_requests > 0:
             line["serving"] = serving_run(args.serve_requests, 2000.0, args.serve_budget_gb)
             # the same stream at an arrival rate the GPU sustains (arrivals spread
@@ -425,6 +531,19 @@ def run_ours(args):
     b.close()
     if dist:
         dist.destroy_process_group()
+
+
+def launch_ranks(n: int) -> int:
+    """Runs this script as n ranks on 127.0.0.1 (torch.distributed.run) and
+    returns their exit status; the ranks read WORLD_SIZE/RANK/LOCAL_RANK."""
+    import socket
+
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
 
 
 def run_reference(args):
@@ -446,10 +565,9 @@ def run_reference(args):
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": args.ref_step_budget * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64 (bitwise) + f64 compare", "data": "synthetic",
-        "config": {"workload": "batched PT mix: 4096 instances x 16 slots, 2D L{16..64} / 3D L{8..24}, "
-                               "bounded sample per step", "slots": 16},
+        "config": c4_config(args, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": per_step[-1]["cores"], "kind": "reference",
-                         "sample": samples},
+                         "sample": "per step: " + samples, "per_core": value / per_step[-1]["cores"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -544,7 +662,11 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-step-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--plain-budget", type=float, default=8.0, help="seconds of the plain form (0 = skip)")
+    ap.add_argument("--plain-instances", type=int, default=100,
+                    help="instances of the plain one-instance-per-launch sample (0 = skip)")
+    ap.add_argument("--plain-budget", type=float, default=6.0,
+                    help="seconds of the host-driven plain form (0 = skip)")
+    ap.add_argument("--cpu-stub", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--serve-requests", type=int, default=None,
                     help="requests in the serving sample (0 = skip; default 300, or 20,000 for --workload serve)")
     ap.add_argument("--serve-budget-gb", type=float, default=16.0)
@@ -553,6 +675,10 @@ def main():
                     help="arrivals/s of the default line's second serving sample")
     ap.add_argument("--workload", choices=["c4", "serve", "c1", "c2", "c3"], default="c4")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args.gpus))
+    if args.cpu_stub:
+        return run_stub(args)
     if args.serve_requests is None and args.workload == "c4":
         args.serve_requests = 300
     if args.workload != "c4" and args.impl == "ours":

@@ -35,8 +35,11 @@ _vp = ctypes.c_void_p
 
 
 def build() -> None:
-    """Compile the oracle (and the reference library where its sources exist)."""
-    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile")], check=True)
+    """Compile the oracle, and the reference library when SA_REFERENCE_SRC names
+    the reference's src/ directory."""
+    ref = os.environ.get("SA_REFERENCE_SRC")
+    extra = [f"REF_SRC={ref}"] if ref else []
+    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile"), *extra], check=True)
 
 
 def _ptr(a: np.ndarray, ct):
@@ -114,6 +117,7 @@ def ref_lib():
     global _REF
     if _REF is None:
         lib = ctypes.CDLL(REF_SO)
+        lib.ref_omp_threads.argtypes = [ctypes.c_int]
         lib.ref_sys_new.restype = _vp
         lib.ref_sys_new.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]
         lib.ref_sys_free.argtypes = [_vp]

@@ -20,6 +20,8 @@
 #include <string>
 #include <vector>
 
+#include <omp.h>
+
 #include "annealing.hpp"
 #include "cpu_2d.hpp"
 #include "cpu_2dp.hpp"
@@ -77,6 +79,11 @@ struct RefPT {
 }  // namespace
 
 extern "C" {
+
+// OpenMP threads of the calling host thread's parallel regions (the PT
+// template's loop over slots, src/parallel_tempering.hpp:86). The CPU baseline
+// runs one instance per host thread with 1, so the cores go to instances.
+void ref_omp_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
 
 void* ref_sys_new(int kind, int L, double T, double h) {
   RefSys* r = new RefSys();

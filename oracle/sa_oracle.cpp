@@ -278,6 +278,21 @@ uint32_t sao_philox_draw(uint64_t seed, uint64_t subseq, uint64_t index) {
   return philox_draw(seed, subseq, index);
 }
 float sao_uniform_from_u32(uint32_t u) { return uniform_from_u32(u); }
+
+// Draws 0..ndraws-1 of subsequences 0..nsubs-1 of key `seed` and the bit
+// patterns of their uniforms, laid out [subsequence][draw] (the layout of
+// tests/golden/gen_curand_golden.cu --bulk).
+void sao_philox_bulk(uint64_t seed, long nsubs, long ndraws, uint32_t* u32_out, uint32_t* uni_out) {
+  for (long s = 0; s < nsubs; ++s)
+    for (long k = 0; k < ndraws; ++k) {
+      const uint32_t u = philox_draw(seed, (uint64_t)s, (uint64_t)k);
+      const float f = uniform_from_u32(u);
+      uint32_t bits;
+      memcpy(&bits, &f, 4);
+      u32_out[s * ndraws + k] = u;
+      uni_out[s * ndraws + k] = bits;
+    }
+}
 uint64_t sao_threshold(float b) { return threshold_of(b); }
 
 // Exhaustive: uniform_from_u32 is non-decreasing over all 2^32 inputs, lies in

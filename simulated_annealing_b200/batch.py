@@ -239,33 +239,3 @@ class Batch:
             self.close()
         except Exception:
             pass
-
-
-def smoke_check() -> None:
-    """A tiny mixed batch (one 2D and one 3D PT ensemble) against the oracle."""
-    from oracle import oracle as O
-
-    b = Batch()
-    lad = b.add_ladder([0.6, 1.0, 1.6, 2.2])
-    specs = [(O.LAT_2D, 8, 7), (O.LAT_3D, 4, 9)]
-    for lat, L, seed in specs:
-        b.add_instance(lat, L, ladder=lad, seed_J=seed, seed=seed + 100)
-    b.finalize()
-    b.record_exchanges(16)
-    b.run(6)
-    b.sync()
-    for i, (lat, L, seed) in enumerate(specs):
-        systems = [O.OracleSystem(lat, L, mode=O.MODE_PHILOX) for _ in range(4)]
-        for s in systems:
-            s.set_seed(seed)
-            s.init_J()
-            s.set_seed(seed + 100)
-            s.init_rand()
-        pt = O.OraclePT(systems, [0.6, 1.0, 1.6, 2.2], 1)
-        steps = [pt.step(0) for _ in range(6)]
-        pairs, masks = b.exchanges(i)
-        assert [p for p, _, _ in steps] == pairs.tolist(), "exchange pairs differ from the oracle"
-        assert [m for _, m, _ in steps] == [int(m) for m in masks], "exchange masks differ from the oracle"
-        for slot, s in enumerate(systems):
-            assert np.array_equal(b.spins(i, slot), s.spins()), "batched spins differ from the oracle"
-    b.close()

@@ -1,6 +1,6 @@
 // Fixture generator: records what the CUDA toolkit's cuRAND device API returns
 // for the Philox4_32_10 generator, so that the oracle's own Philox restatement
-// (oracle/sa_oracle.c) can be pinned against it without a GPU.
+// (oracle/sa_oracle.cpp) can be pinned against it without a GPU.
 //
 // The reference seeds one Philox state per lattice site with
 // curand_init(seed, site, 0, &state) (src/random.cu:15-23), draws the coupling
@@ -12,7 +12,14 @@
 //   nvcc -gencode arch=compute_100a,code=sm_100a -O2 -o gen_curand_golden \
 //        tests/golden/gen_curand_golden.cu
 //   ./gen_curand_golden > tests/golden/curand_philox_golden.json
+//   ./gen_curand_golden --bulk curand_bulk.bin
+//   python tests/golden/hash_curand_bulk.py curand_bulk.bin > tests/golden/curand_philox_bulk.json
+// --bulk writes, for each seed of kBulkSeeds, the first kBulkDraws curand()
+// outputs and the first kBulkDraws curand_uniform() bit patterns of every
+// subsequence 0..kBulkSubs-1 (offset 0), as little-endian u32:
+// [seed][u32 | uniform][subsequence][draw].
 #include <cstdio>
+#include <cstring>
 #include <cstdint>
 #include <vector>
 #include <cuda_runtime.h>
@@ -23,6 +30,23 @@ struct Case {
 };
 
 constexpr int kDraws = 20;
+constexpr int kBulkSubs = 4096, kBulkDraws = 64;
+const unsigned long long kBulkSeeds[] = {1ULL, 2ULL, 3ULL, 4ULL, 1234ULL, 1000ULL, 1001ULL, 1002ULL, 1003ULL};
+
+__global__ void bulk_kernel(unsigned long long seed, unsigned* u32_out, unsigned* uni_out) {
+  int sub = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sub >= kBulkSubs) return;
+  curandStatePhilox4_32_10_t a, b;
+  curand_init(seed, (unsigned long long)sub, 0ULL, &a);
+  curand_init(seed, (unsigned long long)sub, 0ULL, &b);
+  for (int k = 0; k < kBulkDraws; ++k) {
+    u32_out[sub * kBulkDraws + k] = curand(&a);
+    const float f = curand_uniform(&b);
+    unsigned bits;
+    memcpy(&bits, &f, 4);
+    uni_out[sub * kBulkDraws + k] = bits;
+  }
+}
 
 __global__ void draw_kernel(const Case* cases, int n, unsigned* u32_out,
                             float* uni_out) {
@@ -46,7 +70,34 @@ __global__ void draw_kernel(const Case* cases, int n, unsigned* u32_out,
     }                                                                      \
   } while (0)
 
-int main() {
+static int bulk(const char* path) {
+  const size_t per = (size_t)kBulkSubs * kBulkDraws;
+  unsigned *d_u, *d_f;
+  CK(cudaMalloc(&d_u, per * sizeof(unsigned)));
+  CK(cudaMalloc(&d_f, per * sizeof(unsigned)));
+  FILE* out = fopen(path, "wb");
+  if (!out) {
+    fprintf(stderr, "cannot open %s\n", path);
+    return 1;
+  }
+  std::vector<unsigned> h(per);
+  for (unsigned long long seed : kBulkSeeds) {
+    bulk_kernel<<<kBulkSubs / 128, 128>>>(seed, d_u, d_f);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(h.data(), d_u, per * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    fwrite(h.data(), sizeof(unsigned), per, out);
+    CK(cudaMemcpy(h.data(), d_f, per * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    fwrite(h.data(), sizeof(unsigned), per, out);
+  }
+  fclose(out);
+  cudaFree(d_u);
+  cudaFree(d_f);
+  return 0;
+}
+
+int main(int argc, char** argv) {
+  if (argc == 3 && strcmp(argv[1], "--bulk") == 0) return bulk(argv[2]);
   std::vector<Case> cases;
   const unsigned long long seeds[] = {0ULL, 1ULL, 2ULL, 3ULL, 4ULL, 1234ULL,
                                       1000ULL, 1001ULL, 1002ULL, 1003ULL,

@@ -57,6 +57,25 @@ def test_mt_stream_matches_reference_classes(sab, lat, L, T, h):
     _same(g, r)
 
 
+@pytest.mark.parametrize("lat,L", [(O.LAT_2D, 32), (O.LAT_2D, 64), (O.LAT_2D_OPEN_X, 64), (O.LAT_3D, 16),
+                                   (O.LAT_3D, 32)])
+def test_mt_large_lattices_match_reference_classes(sab, lat, L):
+    """The configurations' lattice sizes in the reference's random stream."""
+    g, r = _mt(lat, L, 1.0), O.RefSystem(lat, L, 1.0)
+    for x in (g, r):
+        x.set_seed(3)
+        x.init_J()
+        x.set_seed(4)
+        x.init_rand()
+    _same(g, r)
+    for n, T in ((1, 1.0), (9, 1.0), (40, 0.4)):
+        g.set_T(T)
+        r.set_T(T)
+        g.sweep(n)
+        r.sweep(n)
+        _same(g, r)
+
+
 @pytest.mark.parametrize("lat,L", [(O.LAT_2D, 8), (O.LAT_3D, 4), (O.LAT_2D_OPEN_X, 6)])
 def test_mt_anneal_matches_reference_template(sab, lat, L):
     """annealing<> (geometric cooling, measure every sweep) on the reference

@@ -77,3 +77,27 @@ def test_shard_bounds():
     with pytest.raises(AssertionError):
         bench.shard_instances(2, 2, 4)
     assert bench.shard_instances(1, 4, 3) == bench.c4_instances(12)[3:6]
+
+
+def test_bench_gpus_flag_launches_ranks():
+    """`bench.py --gpus 2` with no torchrun environment starts its two ranks
+    itself (torch.distributed.run on 127.0.0.1); the GPU leg is replaced by
+    the stub leg (gloo), which keeps the sharding and the max-over-ranks
+    reduction. Rank 0 prints one line for the whole job."""
+    import json
+    import subprocess
+    import sys
+
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--cpu-stub",
+                        "--instances", "8"], capture_output=True, text=True, timeout=300, env=env, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert d["n_gpus"] == 2 and d["instances_total"] == 16
+    assert d["ms_per_step"] == 11.0  # rank 1's stand-in time: the slower rank
+    assert d["seed_sum"] == float(sum(s for _, _, s in bench.c4_instances(16)))

@@ -9,6 +9,7 @@ import os
 import struct
 
 import numpy as np
+import pytest
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "curand_philox_golden.json")
 
@@ -57,3 +58,28 @@ def test_threshold_definition(oracle):
         assert not (oracle.uniform_from_u32(t) < b)
         for u in rng.integers(0, 1 << 32, 200):
             assert (oracle.uniform_from_u32(int(u)) < b) == (int(u) < t)
+
+
+BULK = os.path.join(os.path.dirname(__file__), "golden", "curand_philox_bulk.json")
+
+
+@pytest.mark.skipif(not os.path.exists(BULK), reason="bulk cuRAND digests not generated")
+def test_philox_bulk_matches_curand(oracle):
+    """Subsequences 0..4095 x draws 0..63 for nine seeds (2.36 M draws and
+    their uniforms), as SHA-256 digests of cuRAND's outputs on a B200."""
+    import ctypes
+    import hashlib
+
+    g = json.load(open(BULK))
+    subs, draws = g["subsequences"], g["draws"]
+    lib = oracle.oracle_lib()
+    lib.sao_philox_bulk.argtypes = [ctypes.c_uint64, ctypes.c_long, ctypes.c_long,
+                                    ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]
+    assert len(g["seeds"]) == 9
+    for seed, h in g["seeds"].items():
+        u = np.zeros(subs * draws, dtype="<u4")
+        f = np.zeros(subs * draws, dtype="<u4")
+        lib.sao_philox_bulk(int(seed), subs, draws, u.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                            f.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+        assert hashlib.sha256(u.tobytes()).hexdigest() == h["u32_sha256"], seed
+        assert hashlib.sha256(f.tobytes()).hexdigest() == h["uniform_bits_sha256"], seed

@@ -39,6 +39,27 @@ def test_sweep_and_measure_match_reference(lat, L, T, h):
         assert np.array_equal(r.measure_float(), o.measure_float())
 
 
+@pytest.mark.parametrize("lat,L", [(O.LAT_2D, 32), (O.LAT_2D, 64), (O.LAT_2D_OPEN_X, 64), (O.LAT_3D, 16),
+                                   (O.LAT_3D, 32)])
+def test_large_lattices_match_reference(lat, L):
+    """The configurations' lattice sizes (2D L=32/64, 3D L=16/32): spins and
+    float energies after 1, 10 and 25 sweeps, at two temperatures."""
+    r = O.RefSystem(lat, L, 1.0, 0.0)
+    o = O.OracleSystem(lat, L, 1.0, 0.0, O.MODE_MT)
+    for x in (r, o):
+        x.set_seed(3)
+        x.init_J()
+        x.set_seed(4)
+        x.init_rand()
+    for n, T in ((1, 1.0), (9, 1.0), (15, 0.4)):
+        r.set_T(T)
+        o.set_T(T)
+        r.sweep(n)
+        o.sweep(n)
+        assert np.array_equal(r.state()[0], o.spins())
+        assert np.array_equal(r.measure_float(), o.measure_float())
+
+
 def test_init_order_and_swap_match_reference():
     a, b = O.RefSystem(O.LAT_3D, 4), O.RefSystem(O.LAT_3D, 4)
     c, d = O.OracleSystem(O.LAT_3D, 4, mode=O.MODE_MT), O.OracleSystem(O.LAT_3D, 4, mode=O.MODE_MT)
