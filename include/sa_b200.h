@@ -149,10 +149,31 @@ int sa_sys_save(sa_system_t sys, void* buf, size_t cap, size_t* len);
 int sa_sys_load(sa_system_t sys, const void* buf, size_t len);
 
 /* The exchange schedule of parallel_tempering<> for n temperatures
- * (src/parallel_tempering.hpp:193-198, 251-253): std::mt19937(123) driving
- * uniform_int_distribution<int>(0, n-2) then uniform_real_distribution<double>;
- * entries skip .. skip+count-1 into pair[] and r[] (host). */
+ * (src/parallel_tempering.hpp:28-30, :59, :112-114): std::mt19937(123)
+ * driving uniform_int_distribution<int>(0, n-2) then
+ * uniform_real_distribution<double>; entries skip .. skip+count-1 into pair[]
+ * and r[] (host). */
 int sa_pt_sequence(int n, long skip, long count, int32_t* pair, double* r);
+
+/* The same generator as an object that keeps its position, for drivers that
+ * draw one attempt at a time and for checkpoints: the members gen, uni_int
+ * and uni_double of parallel_tempering<> (src/parallel_tempering.hpp:28-30),
+ * created as its constructor creates them (:59) for n temperatures. */
+typedef struct sa_pt_gen* sa_pt_gen_t;
+int sa_pt_gen_create(int n, sa_pt_gen_t* out);
+int sa_pt_gen_destroy(sa_pt_gen_t g);
+/* The next `count` attempts (src/parallel_tempering.hpp:112-114): pair[k] =
+ * uni_int(gen), then r[k] = uni_double(gen). */
+int sa_pt_gen_next(sa_pt_gen_t g, long count, int32_t* pair, double* r);
+/* update_T's widening of the pair range by one (src/parallel_tempering.hpp:
+ * 410): uni_int becomes uniform_int_distribution<int>(a, b+1). */
+int sa_pt_gen_widen(sa_pt_gen_t g);
+/* The three objects' bytes as parallel_tempering<>::save writes them, in its
+ * order gen, uni_int, uni_double (src/parallel_tempering.hpp:284-287; the
+ * raw libstdc++ objects, 5024 bytes on LP64); load takes the same bytes
+ * (:324-327). buf == NULL: *len receives the size. */
+int sa_pt_gen_save(sa_pt_gen_t g, void* buf, size_t cap, size_t* len);
+int sa_pt_gen_load(sa_pt_gen_t g, const void* buf, size_t len);
 /* The reference's exchange mask for one pair (src/parallel_tempering.hpp:
  * 141-162): bit j iff dE*dB > 0 || r < exp(dB*dE), dE = -(Ei[j]-Ej[j]) (float),
  * dB = 1/Ti - 1/Tj. Host-only arithmetic. */

@@ -134,11 +134,19 @@ def ref_lib():
         lib.ref_pt_new.restype = _vp
         lib.ref_pt_new.argtypes = [ctypes.POINTER(_vp), _f64p, ctypes.c_int, ctypes.c_long]
         lib.ref_pt_step.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _u64p]
+        lib.ref_pt_last_T.restype = ctypes.c_double
+        lib.ref_pt_last_T.argtypes = [_vp]
+        lib.ref_pt_update_T.argtypes = [_vp]
+        lib.ref_pt_save.restype = ctypes.c_long
+        lib.ref_pt_save.argtypes = [_vp, ctypes.c_char_p, ctypes.c_long]
+        lib.ref_pt_load.argtypes = [_vp, ctypes.c_char_p, ctypes.c_long]
         lib.ref_pt_print_swap.restype = ctypes.c_int
         lib.ref_pt_print_swap.argtypes = [_vp, ctypes.c_char_p, ctypes.c_int]
         lib.ref_pt_free.argtypes = [_vp]
         lib.ref_anneal_run.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, _f32p]
+        lib.ref_save_J.argtypes = [_vp, ctypes.c_char_p]
+        lib.ref_load_J.argtypes = [_vp, ctypes.c_char_p]
         lib.ref_save.restype = ctypes.c_long
         lib.ref_save.argtypes = [_vp, ctypes.c_char_p, ctypes.c_long]
         lib.ref_load.argtypes = [_vp, ctypes.c_char_p, ctypes.c_long]
@@ -344,6 +352,12 @@ class RefSystem:
     def swap(self, other, mask):
         self.lib.ref_swap(self.h, other.h, mask)
 
+    def save_J(self, fname: str) -> None:
+        self.lib.ref_save_J(self.h, fname.encode())
+
+    def load_J(self, fname: str) -> None:
+        self.lib.ref_load_J(self.h, fname.encode())
+
     def save(self) -> bytes:
         n = self.lib.ref_save(self.h, None, 0)
         buf = ctypes.create_string_buffer(n)
@@ -379,6 +393,21 @@ class RefPT:
         mask = np.zeros(1, dtype=np.uint64)
         self.lib.ref_pt_step(self.h, stride, ctypes.byref(pair), _ptr(mask, _u64p))
         return int(pair.value), int(mask[0])
+
+    def last_T(self) -> float:
+        return float(self.lib.ref_pt_last_T(self.h))
+
+    def update_T(self) -> None:
+        self.lib.ref_pt_update_T(self.h)
+
+    def save(self) -> bytes:
+        n = self.lib.ref_pt_save(self.h, None, 0)
+        buf = ctypes.create_string_buffer(n)
+        self.lib.ref_pt_save(self.h, buf, n)
+        return buf.raw[:n]
+
+    def load(self, data: bytes) -> None:
+        self.lib.ref_pt_load(self.h, data, len(data))
 
     def print_swap(self) -> str:
         buf = ctypes.create_string_buffer(1 << 16)

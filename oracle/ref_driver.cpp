@@ -39,6 +39,7 @@ struct RefSys {
 struct SwapLog {
   std::vector<int> pair;
   std::vector<spin_t> mask;
+  std::vector<double> T;  // temperature of the pair's lower system
 };
 
 class spy_sys : public cpu_sys {
@@ -62,6 +63,7 @@ class spy_sys : public cpu_sys {
   void swap(cpu_sys* other, std::unique_ptr<spin_t[]> mask) override {
     log->pair.push_back(id);
     log->mask.push_back(mask[0]);
+    log->T.push_back(in->get_T());
     in->swap(static_cast<spy_sys*>(other)->in, std::move(mask));
   }
   ostream& save(ostream& s) override { return in->save(s); }
@@ -155,6 +157,22 @@ void ref_pt_step(void* p, int stride, int* pair, uint64_t* mask) {
   *pair = r->log.pair.back();
   *mask = r->log.mask.back();
 }
+// The lower temperature of the last exchange's pair (after update_T the
+// systems' creation indices no longer name pairs).
+double ref_pt_last_T(void* p) { return ((RefPT*)p)->log.T.back(); }
+void ref_pt_update_T(void* p) { ((RefPT*)p)->pt->update_T(); }
+// parallel_tempering<>::save / load streams (the .tempsys checkpoint).
+long ref_pt_save(void* p, char* buf, long cap) {
+  std::stringstream ss;
+  ((RefPT*)p)->pt->save(ss);
+  std::string b = ss.str();
+  if (buf && cap >= (long)b.size()) memcpy(buf, b.data(), b.size());
+  return (long)b.size();
+}
+void ref_pt_load(void* p, const char* buf, long len) {
+  std::stringstream ss(std::string(buf, (size_t)len));
+  ((RefPT*)p)->pt->load(ss);
+}
 int ref_pt_print_swap(void* p, char* buf, int len) {
   std::stringstream ss;
   ((RefPT*)p)->pt->print_swap(ss);
@@ -188,6 +206,11 @@ void ref_anneal_run(void* p, double T0, double alfa, int nsteps, int sweeps, int
   std::stringstream in(line);
   for (int j = 0; j < 64; ++j) in >> min_E[j];
 }
+
+// The reference object's own J file writer and reader (cpu_2dp::save_J /
+// load_J -> save_J_2d / load_J_2d, cpu_3d -> *_3d; src/sys_file.cpp:10-110).
+void ref_save_J(void* p, const char* fname) { ((RefSys*)p)->sys->save_J(std::string(fname)); }
+void ref_load_J(void* p, const char* fname) { ((RefSys*)p)->sys->load_J(std::string(fname)); }
 
 // The reference object's own save() / load() byte stream (its checkpoint
 // record), for comparing this engine's record with it.

@@ -377,7 +377,6 @@ template <int P, int SL, int LAT, bool CL, bool SEG = false>
 __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG>(), 1) k_resident(BatchParams p) {
   extern __shared__ __align__(16) word_t s_spins[];
   __shared__ unsigned s_cnt[2][64];   // this CTA's partial counts
-  __shared__ unsigned s_tot[2][64];   // cluster totals
   __shared__ unsigned s_mask[2];
   cg::cluster_group cluster = cg::this_cluster();
   const int C = CL ? (int)cluster.num_blocks() : 1;
@@ -512,6 +511,12 @@ __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG>(), 1) k_resid
   };
   __syncthreads();
   for (int64_t i = 0; i < n; ++i) {
+    // The exchange / measurement counters of this sweep start at zero. The
+    // previous sweep's readers (every CTA of the cluster) finished before its
+    // last cluster barrier, and this sweep's half-sweep barriers separate
+    // these stores from the next counts.
+    for (int t = threadIdx.x; t < 128; t += blockDim.x) (&s_cnt[0][0])[t] = 0;
+    bool hist_now = false;  // a histogram pass used s_cnt in this sweep
     // this sweep's exchange decision, fetched before the half-sweeps hide its latency
     const bool xchg = d.ladder >= 0 && d.nslots > 1 && (sweeps + 1) % p.xinterval == 0;
     Decision dc = {0, 0, 0, 0};
@@ -564,6 +569,7 @@ __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG>(), 1) k_resid
     // energy histograms of every slot, taken before the exchange (the energies
     // the reference's PT step measures, src/parallel_tempering.hpp:85-95)
     if (p.hist && d.hist_off >= 0 && sweeps % p.hstride == 0) {
+      hist_now = true;
       for (int a = 0; a < d.nslots; a += 2) {
         const int nh = (a + 1 < d.nslots) ? 2 : 1;
         rmeasure<CL>(x, d3, open, a, nh, s_cnt);
@@ -594,23 +600,27 @@ __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG>(), 1) k_resid
         a = dc.pair;
         nsl = 2;
       }
-      if constexpr (P == 1 && SL == 1) rmeasure<CL, 4>(x, d3, open, a, nsl, s_cnt);
-      else rmeasure<CL>(x, d3, open, a, nsl, s_cnt);
+      // s_cnt was zeroed at the start of this sweep unless a histogram pass
+      // used it since; four units' loads in flight per lane
+      rmeasure<CL, 4>(x, d3, open, a, nsl, s_cnt, hist_now);
       sync_all();
-      if (threadIdx.x < 128) {
-        unsigned v = 0;
-        if (CL) {
-          for (int r = 0; r < C; ++r) v += cluster.map_shared_rank(&s_cnt[0][0], (unsigned)r)[threadIdx.x];
-        } else {
-          v = (&s_cnt[0][0])[threadIdx.x];
-        }
-        (&s_tot[0][0])[threadIdx.x] = v;
-      }
-      __syncthreads();
       if (xchg) {
+        // every CTA of the cluster reaches the same decision from the
+        // cluster's totals: 64 threads, one replica each, then one barrier
         if (threadIdx.x < 64) {
           const int j = threadIdx.x;
-          const int64_t dE = 2 * ((int64_t)s_tot[1][j] - (int64_t)s_tot[0][j]);
+          unsigned v0 = 0, v1 = 0;
+          if (CL) {
+            for (int r = 0; r < C; ++r) {
+              const unsigned* rc = cluster.map_shared_rank(&s_cnt[0][0], (unsigned)r);
+              v0 += rc[j];
+              v1 += rc[64 + j];
+            }
+          } else {
+            v0 = s_cnt[0][j];
+            v1 = s_cnt[1][j];
+          }
+          const int64_t dE = 2 * ((int64_t)v1 - (int64_t)v0);
           const bool acc = dE >= dc.lo && dE <= dc.hi;
           const unsigned bal = __ballot_sync(0xffffffffu, acc);
           if (lane == 0) s_mask[threadIdx.x >> 5] = bal;
@@ -638,7 +648,13 @@ __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG>(), 1) k_resid
         }
         xsteps += 1;
       } else if (q == 0 && threadIdx.x < 64) {
-        const int64_t e = 2 * (int64_t)s_tot[0][threadIdx.x] - d.nbonds;
+        unsigned v = 0;
+        if (CL) {
+          for (int r = 0; r < C; ++r) v += cluster.map_shared_rank(&s_cnt[0][0], (unsigned)r)[threadIdx.x];
+        } else {
+          v = s_cnt[0][threadIdx.x];
+        }
+        const int64_t e = 2 * (int64_t)v - d.nbonds;
         my_elast = e;
         my_emax = (measured == 0) ? e : max(my_emax, e);
       }

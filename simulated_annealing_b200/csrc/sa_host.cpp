@@ -197,7 +197,7 @@ void pt_accept_interval(double dB, double r, int64_t span, int64_t* lo, int64_t*
 extern "C" const char* sa_last_error(void) { return sa::g_last_error.c_str(); }
 
 // The exchange sequence of parallel_tempering<> (src/parallel_tempering.hpp:
-// 193-198, 251-253): std::mt19937 gen(123); per step i = uni_int(gen) from
+// 28-30, :59, :112-114): std::mt19937 gen(123); per step i = uni_int(gen) from
 // uniform_int_distribution<int>(0, n-2), then r = uni_double(gen) from
 // uniform_real_distribution<double>(0, 1) -- libstdc++'s own generators.
 extern "C" int sa_pt_sequence(int n, long skip, long count, int32_t* pair, double* r) {
@@ -214,6 +214,68 @@ extern "C" int sa_pt_sequence(int n, long skip, long count, int32_t* pair, doubl
       r[k - skip] = u;
     }
   }
+  return SA_OK;
+}
+
+// The exchange generator as an object (the template's gen / uni_int /
+// uni_double members). Its checkpoint bytes are the raw objects, as the
+// template's save() writes them: libstdc++'s std::mt19937 (624 state words
+// of uint_fast32_t and the position), then the two distributions' parameters.
+struct sa_pt_gen {
+  std::mt19937 gen{123};
+  std::uniform_int_distribution<int> uni_int;
+  std::uniform_real_distribution<double> uni_double{0., 1.};
+  explicit sa_pt_gen(int n) : uni_int(0, n - 2) {}
+};
+
+extern "C" int sa_pt_gen_create(int n, sa_pt_gen_t* out) {
+  if (n < 2 || !out) return sa::fail(SA_ERR_INVALID, "sa_pt_gen_create: need n >= 2 and an output");
+  *out = new sa_pt_gen(n);
+  return SA_OK;
+}
+
+extern "C" int sa_pt_gen_destroy(sa_pt_gen_t g) {
+  delete g;
+  return SA_OK;
+}
+
+extern "C" int sa_pt_gen_next(sa_pt_gen_t g, long count, int32_t* pair, double* r) {
+  if (!g || count < 0 || (count > 0 && (!pair || !r))) return sa::fail(SA_ERR_INVALID, "bad arguments to sa_pt_gen_next");
+  for (long k = 0; k < count; ++k) {
+    pair[k] = g->uni_int(g->gen);
+    r[k] = g->uni_double(g->gen);
+  }
+  return SA_OK;
+}
+
+extern "C" int sa_pt_gen_widen(sa_pt_gen_t g) {
+  if (!g) return sa::fail(SA_ERR_INVALID, "null generator");
+  g->uni_int = std::uniform_int_distribution<int>(g->uni_int.a(), g->uni_int.b() + 1);
+  return SA_OK;
+}
+
+static constexpr size_t kPtGenBytes =
+    sizeof(std::mt19937) + sizeof(std::uniform_int_distribution<int>) + sizeof(std::uniform_real_distribution<double>);
+
+extern "C" int sa_pt_gen_save(sa_pt_gen_t g, void* buf, size_t cap, size_t* len) {
+  if (!g || !len) return sa::fail(SA_ERR_INVALID, "null argument");
+  *len = kPtGenBytes;
+  if (!buf) return SA_OK;
+  if (cap < kPtGenBytes) return sa::fail(SA_ERR_BUFFER, "buffer too small");
+  char* p = (char*)buf;
+  memcpy(p, &g->gen, sizeof g->gen);
+  memcpy(p + sizeof g->gen, &g->uni_int, sizeof g->uni_int);
+  memcpy(p + sizeof g->gen + sizeof g->uni_int, &g->uni_double, sizeof g->uni_double);
+  return SA_OK;
+}
+
+extern "C" int sa_pt_gen_load(sa_pt_gen_t g, const void* buf, size_t len) {
+  if (!g || !buf) return sa::fail(SA_ERR_INVALID, "null argument");
+  if (len != kPtGenBytes) return sa::fail(SA_ERR_MISMATCH, "generator record has the wrong size");
+  const char* p = (const char*)buf;
+  memcpy(&g->gen, p, sizeof g->gen);
+  memcpy(&g->uni_int, p + sizeof g->gen, sizeof g->uni_int);
+  memcpy(&g->uni_double, p + sizeof g->gen + sizeof g->uni_int, sizeof g->uni_double);
   return SA_OK;
 }
 

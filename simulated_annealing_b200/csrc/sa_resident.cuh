@@ -894,15 +894,20 @@ __device__ __forceinline__ void rmeasure_body(const ResCtx& x, bool d3, bool ope
 }
 
 // Partial satisfied-bond counts of slots a..a+nsl-1 (nsl 1 or 2) over this
-// CTA's sites into cnt[q][j] (zeroed here). Five counter planes per lane: a
+// CTA's sites added into cnt[q][j] (zeroed here first when `clear`; else the
+// caller zeroed it before a barrier). Five counter planes per lane: a
 // batched ensemble's share of a warp fits in one chunk (one warp sum per
 // measurement); a single-slot lattice spread over few warps takes a warp
 // sum every 10 (3D) or 15 (2D) units, which keeps the counters in registers.
+// UNR units are formed before any is added, so their loads (couplings from
+// L2 above all) are in flight together.
 template <bool CL, int UNR = 1>
 __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, int a, int nsl,
-                                         unsigned (*cnt)[64]) {
-  for (int i = threadIdx.x; i < 128; i += blockDim.x) (&cnt[0][0])[i] = 0;
-  __syncthreads();
+                                         unsigned (*cnt)[64], bool clear = true) {
+  if (clear) {
+    for (int i = threadIdx.x; i < 128; i += blockDim.x) (&cnt[0][0])[i] = 0;
+    __syncthreads();
+  }
   if (nsl == 2) rmeasure_body<CL, UNR, 2, 5>(x, d3, open, a, cnt);
   else rmeasure_body<CL, UNR, 1, 5>(x, d3, open, a, cnt);
 }

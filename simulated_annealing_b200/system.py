@@ -21,6 +21,44 @@ def _p(a: np.ndarray, ct=ctypes.c_uint64):
     return a.ctypes.data_as(ctypes.POINTER(ct))
 
 
+def read_J_file(fname: str, dim: int, N: int):
+    """The reference's J file (load_J_2d / load_J_3d, src/sys_file.cpp:10-35,
+    :60-88): int dim; long N; then Jx[2N], Jy[2N] (and Jz[2N]) as raw
+    little-endian words, no padding. Raises ValueError where the reference
+    returns -1 (cannot open), -2 (other dimension) or -3 (other N)."""
+    try:
+        f = open(fname, "rb")
+    except OSError as e:
+        raise ValueError(f"cannot open J file {fname}") from e
+    with f:
+        head = f.read(12)
+        if len(head) < 12:
+            raise ValueError(f"J file {fname} is truncated")
+        d, n = struct.unpack("<iq", head)
+        if d != dim:
+            raise ValueError(f"J file is {d}D, system is {dim}D")
+        if n != N:
+            raise ValueError(f"J file has N={n}, system has N={N}")
+        arrs = []
+        for _ in range(dim):
+            b = f.read(16 * N)
+            if len(b) != 16 * N:
+                raise ValueError(f"J file {fname} is truncated")
+            arrs.append(np.frombuffer(b, dtype="<u8").astype(np.uint64))
+    return tuple(arrs)
+
+
+def write_J_file(fname: str, arrays) -> None:
+    """Writes the reference's J file (save_J_2d / save_J_3d,
+    src/sys_file.cpp:37-58, :90-110) from the reference-layout couplings."""
+    arrays = [np.ascontiguousarray(a, dtype="<u8") for a in arrays]
+    N = arrays[0].size // 2
+    with open(fname, "wb") as f:
+        f.write(struct.pack("<iq", len(arrays), N))
+        for a in arrays:
+            f.write(a.tobytes())
+
+
 class GpuSystem:
     """One lattice x 64 replicas on the GPU (gpu_2d / gpu_3d replacement)."""
 
@@ -103,23 +141,12 @@ class GpuSystem:
         m = int(mask[0]) if hasattr(mask, "__len__") else int(mask)
         check(self._lib.sa_sys_swap(self._h, other._h, m & 0xFFFFFFFFFFFFFFFF))
 
-    # J files: int dim; long N; Jx[2N]; Jy[2N]; (Jz[2N])  (src/sys_file.cpp:10-110)
+    # J files (src/sys_file.cpp:10-110): see read_J_file / write_J_file
     def load_J(self, fname: str) -> None:
-        with open(fname, "rb") as f:
-            d, n = struct.unpack("<iq", f.read(12))
-            if d != self.dim:
-                raise ValueError(f"J file is {d}D, system is {self.dim}D")
-            if n != self.N:
-                raise ValueError(f"J file has N={n}, system has N={self.N}")
-            arrs = [np.frombuffer(f.read(16 * self.N), dtype=np.uint64) for _ in range(self.dim)]
-        self.set_J(*arrs)
+        self.set_J(*read_J_file(fname, self.dim, self.N))
 
     def save_J(self, fname: str) -> None:
-        arrs = self.get_J()
-        with open(fname, "wb") as f:
-            f.write(struct.pack("<iq", self.dim, self.N))
-            for a in arrs:
-                f.write(a.astype(np.uint64).tobytes())
+        write_J_file(fname, self.get_J())
 
     def save_sys(self, prefix: str) -> None:
         """PBM image per replica bit (src/gpu_2d.cu:275-299)."""
@@ -142,6 +169,17 @@ class GpuSystem:
     def load(self, data: bytes) -> None:
         buf = ctypes.create_string_buffer(data, len(data))
         check(self._lib.sa_sys_load(self._h, buf, len(data)))
+
+    def clone(self) -> "GpuSystem":
+        """A copy of this system (cpu_sys::clone, src/cpu_sys.hpp:30): same
+        lattice, temperature, field, random mode and position, spins and
+        couplings, in a new device allocation."""
+        c = GpuSystem(self.lattice, self.L, self.get_T(), self.h)
+        if self.rng_mode() == _lib.SA_RNG_MT19937_64:
+            c.load_reference(self.save_reference())
+        else:
+            c.load(self.save())
+        return c
 
     def save_reference(self) -> bytes:
         """The record cpu_2dp::save / cpu_3d::save write (mt19937_64 mode)."""
