@@ -128,6 +128,14 @@ int sa_sys_get_N(sa_system_t sys, long* N);
  *   Switching to it reseeds the generator with the current seed. */
 int sa_sys_set_rng_mode(sa_system_t sys, int mode);
 int sa_sys_get_rng_mode(sa_system_t sys, int* mode);
+/* The colour of each sweep's first half-sweep (default 0). The reference's
+ * GPU systems hold two lattices and update one from the other
+ * (src/gpu_2d.cu:109-120): of the two configurations they carry, the second
+ * updates its colour-1 sites first (draw t+2n) and its colour-0 sites second
+ * (t+2n+1). Colour 1 gives that order; such a system also draws its initial
+ * spins from a counter range of its own. Philox mode only. */
+int sa_sys_set_first_colour(sa_system_t sys, int colour);
+int sa_sys_get_first_colour(sa_system_t sys, int* colour);
 /* The reference CPU classes' own checkpoint record, byte for byte as
  * cpu_2dp::save / cpu_3d::save write it (src/cpu_2dp.cpp:444-456,
  * src/cpu_3d.cpp:449-461): L, T, h, spins, the reference-layout couplings and

@@ -68,6 +68,25 @@ int sa_batch_histogram(sa_batch_t b, int instance, int slot, int32_t* out, long 
 int sa_batch_set_kernel(sa_batch_t b, int kernel);
 /* Kernel launches one sa_batch_run issues (one per launch group). */
 int sa_batch_launches_per_run(sa_batch_t b, int* n);
+/* Launch shapes of the resident kernel. A bucket is (lattice, L, slots); its
+ * shape is seven int32: lattice, L, slots, C (CTAs per instance cluster), SL
+ * (slots per lane: 1, or 2 for an even slot count), warps per block, and 1
+ * for the high-register form of the two-slot 3D walk. No counterpart in the
+ * reference (it launches one system per kernel with a fixed 16x16 / 8x8x8
+ * block); the shapes replace the engine's own launch heuristics.
+ * sa_tuning_table: the built-in table (measured on a B200 by
+ * simulated_annealing_b200/autotune.py); out == NULL reports the count.
+ * sa_batch_set_tuning: before finalize, use these n entries instead (n = 0:
+ * the heuristics only; n < 0: back to the built-in table). Buckets without an
+ * entry, and batches whose clusters were spread over idle SMs, keep the
+ * heuristic shapes. sa_batch_set_spread(b, 0): never spread (full-batch
+ * shapes even for a few instances). sa_batch_instance_shape: after finalize,
+ * the seven values an instance runs with (C = 0: the global-memory kernel,
+ * C = -1: the wide form). */
+int sa_tuning_table(int32_t* out, int cap, int* n);
+int sa_batch_set_tuning(sa_batch_t b, const int32_t* entries, int n);
+int sa_batch_set_spread(sa_batch_t b, int on);
+int sa_batch_instance_shape(sa_batch_t b, int id, int32_t* out);
 /* Sweeps between exchange attempts (the PT template's `steps`; default 1). */
 int sa_batch_set_exchange_interval(sa_batch_t b, int sweeps_per_exchange);
 /* Anneal instances: measure every `stride` sweeps (0 = never; default 1) and

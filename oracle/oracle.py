@@ -76,6 +76,7 @@ def _load_oracle():
     lib.sao_sys_get_draw.restype = _u64
     lib.sao_sys_get_draw.argtypes = [_vp]
     lib.sao_sys_set_draw.argtypes = [_vp, _u64]
+    lib.sao_sys_set_first_colour.argtypes = [_vp, ctypes.c_int]
     for f in ("sao_sys_init_J", "sao_sys_init_rand", "sao_sys_init_order"):
         getattr(lib, f).argtypes = [_vp]
     lib.sao_sys_sweep.argtypes = [_vp, ctypes.c_long]
@@ -217,6 +218,9 @@ class OracleSystem:
 
     def init_order(self):
         self.lib.sao_sys_init_order(self.h)
+
+    def set_first_colour(self, c: int):
+        self.lib.sao_sys_set_first_colour(self.h, c)
 
     def sweep(self, n: int = 1):
         self.lib.sao_sys_sweep(self.h, n)

@@ -143,6 +143,7 @@ struct OSys {
   int mode;
   // PHILOX state: key, next draw index shared by all sites, spin-init epoch
   uint64_t seed, draw, epoch;
+  int first = 0;  // colour of the first half-sweep of a sweep
   // MT state
   std::mt19937_64 gen;
   std::uniform_real_distribution<double> uni;
@@ -231,7 +232,8 @@ static void update_site(OSys& o, long i, const Draw& r) {
 }
 
 static void sweep_once(OSys& o) {
-  for (int offset = 0; offset < 2; ++offset) {
+  for (int pass = 0; pass < 2; ++pass) {
+    const int offset = pass ^ o.first;  // the colour of this half-sweep
     int zmax = (o.dim == 3) ? o.L : 1;
     for (int z = 0; z < zmax; ++z)
       for (int y = 0; y < o.L; ++y)
@@ -240,7 +242,7 @@ static void sweep_once(OSys& o) {
           Draw r;
           if (o.mode == MODE_PHILOX) {
             r.use_float = true;
-            r.rf = uniform_from_u32(philox_draw(o.seed, (uint64_t)i, o.draw + offset));
+            r.rf = uniform_from_u32(philox_draw(o.seed, (uint64_t)i, o.draw + pass));
             r.rd = 0;
           } else {
             r.use_float = false;
@@ -349,6 +351,9 @@ void sao_sys_set_h(void* p, double h) { OSys* o = (OSys*)p; o->h = h; o->tables(
 double sao_sys_get_T(void* p) { return ((OSys*)p)->T; }
 uint64_t sao_sys_get_draw(void* p) { return ((OSys*)p)->draw; }
 void sao_sys_set_draw(void* p, uint64_t d) { ((OSys*)p)->draw = d; }
+// colour of each sweep's first half-sweep (PHILOX mode): 1 is the second
+// configuration of the reference GPU systems' two-lattice pair
+void sao_sys_set_first_colour(void* p, int c) { ((OSys*)p)->first = c ? 1 : 0; }
 
 void sao_sys_init_J(void* p) {
   OSys* o = (OSys*)p;
@@ -385,7 +390,7 @@ void sao_sys_init_rand(void* p) {
     uint32_t key[2] = {(uint32_t)o->seed, (uint32_t)(o->seed >> 32)};
     for (long i = 0; i < o->N; ++i) {
       uint32_t ctr[4] = {(uint32_t)o->epoch, (uint32_t)(o->epoch >> 32), (uint32_t)i,
-                         0x80000000u | (uint32_t)((uint64_t)i >> 32)};
+                         (o->first ? 0xC0000000u : 0x80000000u) | (uint32_t)((uint64_t)i >> 32)};
       uint32_t out[4];
       philox_block(ctr, key, out);
       o->s[i] = (word_t)out[0] | ((word_t)out[1] << 32);

@@ -55,6 +55,10 @@ for _name, _res, _args in [
     ("sa_batch_last_h2d_bytes", _c.c_int, [_vp, _c.POINTER(_c.c_longlong)]),
     ("sa_batch_anneal_result", _c.c_int, [_vp, _c.c_int, _i64p, _lp]),
     ("sa_batch_sweeps_done", _c.c_int, [_vp, _c.c_int, _lp]),
+    ("sa_tuning_table", _c.c_int, [_c.POINTER(_c.c_int32), _c.c_int, _ip]),
+    ("sa_batch_set_tuning", _c.c_int, [_vp, _c.POINTER(_c.c_int32), _c.c_int]),
+    ("sa_batch_set_spread", _c.c_int, [_vp, _c.c_int]),
+    ("sa_batch_instance_shape", _c.c_int, [_vp, _c.c_int, _c.POINTER(_c.c_int32)]),
 ]:
     _lib.register(_name, _res, _args)
 
@@ -112,6 +116,24 @@ class Batch:
     def finalize(self) -> None:
         check(self._lib.sa_batch_finalize(self._h))
         self._final = True
+
+    def set_tuning(self, entries) -> None:
+        """Launch shapes per bucket, rows of (lattice, L, slots, C, SL, warps,
+        hr); None: back to the built-in table; []: heuristics only."""
+        if entries is None:
+            check(self._lib.sa_batch_set_tuning(self._h, None, -1))
+            return
+        a = np.ascontiguousarray(np.asarray(entries, dtype=np.int32).reshape(-1, 7))
+        check(self._lib.sa_batch_set_tuning(self._h, _p(a, _c.c_int32), len(a)))
+
+    def set_spread(self, on: bool) -> None:
+        check(self._lib.sa_batch_set_spread(self._h, int(bool(on))))
+
+    def shape(self, i: int):
+        """(lattice, L, slots, C, SL, warps, hr) instance i runs with."""
+        out = np.zeros(7, dtype=np.int32)
+        check(self._lib.sa_batch_instance_shape(self._h, i, _p(out, _c.c_int32)))
+        return tuple(int(v) for v in out)
 
     def set_exchange_interval(self, k: int) -> None:
         check(self._lib.sa_batch_set_exchange_interval(self._h, int(k)))
@@ -239,3 +261,13 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def tuning_table() -> np.ndarray:
+    """The built-in launch shapes, rows of (lattice, L, slots, C, SL, warps, hr)."""
+    lib = _lib.load()
+    n = _c.c_int()
+    check(lib.sa_tuning_table(None, 0, _c.byref(n)))
+    out = np.zeros((max(n.value, 1), 7), dtype=np.int32)
+    check(lib.sa_tuning_table(_p(out, _c.c_int32), n.value, _c.byref(n)))
+    return out[: n.value]

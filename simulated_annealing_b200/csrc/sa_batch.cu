@@ -366,15 +366,20 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchParams p) {
 // barriers only).
 // Single-slot 3D variants (segmented walk, fused measurement) hold more state
 // per thread: 16 warps at up to 128 registers.
-template <int P, int SL, int LAT, bool SEG>
+template <int P, int SL, int LAT, bool SEG, bool HR = false>
 constexpr int res_max_threads() {
-  return (SEG || (P == 1 && SL == 1 && LAT == SA_LATTICE_3D)) ? kSegMaxThreads : kResMaxThreads;
+  return HR ? kHiRegThreads
+            : (SEG || (P == 1 && SL == 1 && LAT == SA_LATTICE_3D)) ? kSegMaxThreads : kResMaxThreads;
 }
 
 // SEG: single-slot 3D instances spread over many SMs walk their columns in
 // segments (rhalf_3d1s) instead of whole (rhalf_3d1).
-template <int P, int SL, int LAT, bool CL, bool SEG = false>
-__global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG>(), 1) k_resident(BatchParams p) {
+// HR: the high-register form for two slots per lane in 3D: at most
+// kHiRegThreads threads, so each can hold ~170 registers (a two-slot 3D walk
+// keeps twice the words live; where a CTA has work for few warps anyway this
+// trades nothing for no spills).
+template <int P, int SL, int LAT, bool CL, bool SEG = false, bool HR = false>
+__global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG, HR>(), 1) k_resident(BatchParams p) {
   extern __shared__ __align__(16) word_t s_spins[];
   __shared__ unsigned s_cnt[2][64];   // this CTA's partial counts
   __shared__ unsigned s_mask[2];
@@ -805,6 +810,7 @@ struct sa_batch {
   InstDesc* d_inst = nullptr;
   InstState* d_state = nullptr;
   int32_t* d_order = nullptr;
+  std::vector<int32_t> h_order;  // the work order of the last finalize (host copy)
   int32_t* d_work = nullptr;
   word_t* d_spins = nullptr;
   word_t* d_J = nullptr;
@@ -828,6 +834,9 @@ struct sa_batch {
   int64_t e_count = 0;         // sum of nslots*64
   bool force_global = false;   // run every instance in the global-memory kernel
   bool no_wide = false;        // never run an instance wide (sa_wide.cuh)
+  bool no_spread = false;      // keep full-batch launch shapes even when SMs sit idle
+  std::vector<TuneEntry> tuning;  // launch shapes per bucket (empty: the built-in table)
+  bool tuning_set = false;
   int hstride = 0;             // energy histograms every hstride sweeps (0 = off)
   int32_t* d_hist = nullptr;
   int64_t hist_count = 0;
@@ -841,6 +850,8 @@ struct sa_batch {
     int lattice, L;     // resident groups hold one shape each
     int SL, RP;         // resident: slots per lane and lanes per site
     bool seg;           // resident: single-slot 3D walked in column segments
+    bool hr;            // resident: the high-register launch bound (two slots per lane, 3D)
+    const TuneEntry* tune;  // resident: the bucket's tuned shape, or null (heuristic shape)
     bool wide;          // one single-slot 3D anneal spread over the whole GPU (sa_wide.cuh)
     int wide_id;        // wide: the instance
     int wide_slot;      // wide: its scratch block in d_wide
@@ -976,11 +987,47 @@ static void spread_clusters(sa_batch* b) {
   }
 }
 
+// The tuned launch shapes compiled into the library (sa_tuning.inc, written
+// by simulated_annealing_b200/autotune.py from timings on a B200).
+static const TuneEntry kBuiltinTuning[] = {
+#include "sa_tuning.inc"
+    {-1, 0, 0, 0, 0, 0, 0}};
+
+static const std::vector<TuneEntry>& builtin_tuning() {
+  static const std::vector<TuneEntry> t = [] {
+    std::vector<TuneEntry> v;
+    for (const TuneEntry& e : kBuiltinTuning)
+      if (e.lattice >= 0) v.push_back(e);
+    return v;
+  }();
+  return t;
+}
+
+// A tuned shape usable for instance d at cluster size C (the shape's C fits
+// the shared-memory budget, SL = 2 only for an even slot count); else null.
+static const TuneEntry* tune_for(const sa_batch* b, const InstDesc& d) {
+  const std::vector<TuneEntry>& t = b->tuning_set ? b->tuning : builtin_tuning();
+  for (const TuneEntry& e : t) {
+    if (e.lattice != d.lattice || e.L != d.L || e.nslots != d.nslots) continue;
+    if (e.C < 1 || e.C > std::min(16, d.L) || resident_bytes(d, e.C) > kResSmemBudget) return nullptr;
+    if (e.SL != 1 && (e.SL != 2 || d.nslots % 2 != 0)) return nullptr;
+    if (e.warps < 1) return nullptr;
+    return &e;
+  }
+  return nullptr;
+}
+
 static std::vector<int32_t> build_groups(sa_batch* b) {
   // work order: grouped by (kernel, P, C), most expensive first inside a group
   b->cluster_of.resize(b->inst.size());
   for (size_t i = 0; i < b->inst.size(); ++i) b->cluster_of[i] = b->force_global ? 0 : choose_cluster(b->inst[i]);
-  spread_clusters(b);
+  if (b->no_spread) b->spread = false;
+  else spread_clusters(b);
+  // full batches take the tuned cluster size of their bucket
+  if (!b->spread)
+    for (size_t i = 0; i < b->inst.size(); ++i)
+      if (b->cluster_of[i] != 0)
+        if (const TuneEntry* e = tune_for(b, b->inst[i])) b->cluster_of[i] = e->C;
   std::vector<int32_t> order(b->inst.size());
   for (size_t i = 0; i < order.size(); ++i) order[i] = (int32_t)i;
   std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
@@ -1013,9 +1060,12 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
       const long lanes = (long)((d.L + C - 1) / C) * (d.L / 2) * seg_lanes(d.L);
       seg = (lanes + kSegMaxThreads - 1) / kSegMaxThreads <= 3;
     }
+    const TuneEntry* te = (!b->spread && C != 0 && !wide && !seg) ? tune_for(b, d) : nullptr;
+    if (te && te->C != C) te = nullptr;
     const bool same = !wide && !b->groups.empty() && !b->groups.back().wide &&
                       b->groups.back().resident == (C != 0) && b->groups.back().P == d.P &&
                       b->groups.back().C == C && b->groups.back().seg == seg &&
+                      b->groups.back().tune == te &&
                       (C == 0 || (b->groups.back().lattice == d.lattice && b->groups.back().L == d.L));
     if (!same) {
       sa_batch::Group g{};
@@ -1031,7 +1081,19 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
       g.SL = 1;
       g.RP = d.P;
       g.seg = seg;
-      if (C && !wide) {
+      g.hr = false;
+      g.tune = te;
+      if (te) {
+        // the bucket's tuned shape
+        g.SL = te->SL;
+        g.RP = 1;
+        while (g.RP * g.SL < d.nslots) g.RP <<= 1;
+        g.hr = te->SL == 2 && te->hr && d.lattice == SA_LATTICE_3D;
+        const int wmax = g.hr ? kHiRegThreads / 32
+                              : (d.lattice == SA_LATTICE_3D && g.SL == 1 && g.RP == 1) ? kSegMaxThreads / 32
+                                                                                       : kResMaxWarps;
+        g.threads = 32 * std::max(1, std::min(te->warps, wmax));
+      } else if (C && !wide) {
         // warp passes of one half-sweep: 3D walks columns, 32/RP per pass; 2D
         // takes tiles of 32 sites (RP sub-steps of 32/RP sites each). Two slots
         // per lane (16-byte accesses, shared addressing and couplings) when the
@@ -1254,8 +1316,11 @@ static void (*resident_kernel_sl(const sa_batch::Group& g))(BatchParams) {
   const bool cl = g.C > 1;
   if constexpr (P == 1 && SL == 1)
     if (g.seg) return cl ? k_resident<1, 1, SA_LATTICE_3D, true, true> : k_resident<1, 1, SA_LATTICE_3D, false, true>;
-  if (g.lattice == SA_LATTICE_3D)
+  if (g.lattice == SA_LATTICE_3D) {
+    if constexpr (SL == 2)
+      if (g.hr) return cl ? k_resident<P, 2, SA_LATTICE_3D, true, false, true> : k_resident<P, 2, SA_LATTICE_3D, false, false, true>;
     return cl ? k_resident<P, SL, SA_LATTICE_3D, true> : k_resident<P, SL, SA_LATTICE_3D, false>;
+  }
   if (g.lattice == SA_LATTICE_2D_OPEN_X)
     return cl ? k_resident<P, SL, SA_LATTICE_2D_OPEN_X, true> : k_resident<P, SL, SA_LATTICE_2D_OPEN_X, false>;
   return cl ? k_resident<P, SL, SA_LATTICE_2D, true> : k_resident<P, SL, SA_LATTICE_2D, false>;
@@ -1369,7 +1434,7 @@ static int group_dispatch(sa_batch* b, const sa_batch::Group& g, int gi, long ns
     size_t lim = 0;
     for (const auto& o : b->groups)
       if (o.resident && o.P == g.P && o.SL == g.SL && o.RP == g.RP && o.lattice == g.lattice &&
-          (o.C > 1) == (g.C > 1))
+          (o.C > 1) == (g.C > 1) && o.hr == g.hr)
         lim = std::max(lim, o.smem);
     return prepare_resident<P>(g, lim, max_clusters);
   }
@@ -1556,6 +1621,7 @@ int sa_batch_finalize(sa_batch_t b) {
     SA_CUDA_TRY(cudaMemsetAsync(b->d_hist, 0, b->hist_count * sizeof(int32_t), b->stream));
   }
   std::vector<int32_t> order = build_groups(b);
+  b->h_order = order;
   if (int st = ensure_wide_scratch(b)) return st;
   const size_t ni = b->inst.size();
   SA_CUDA_TRY(cudaMalloc(&b->d_inst, ni * sizeof(InstDesc)));
@@ -1646,6 +1712,63 @@ int sa_batch_set_kernel(sa_batch_t b, int kernel) {
   b->force_global = (kernel == 1);
   b->no_wide = (kernel == 2);
   return SA_OK;
+}
+
+int sa_batch_set_spread(sa_batch_t b, int on) {
+  if (!b) return fail(SA_ERR_INVALID, "null batch");
+  if (b->finalized) return fail(SA_ERR_INVALID, "set spreading before finalize");
+  b->no_spread = !on;
+  return SA_OK;
+}
+
+int sa_batch_set_tuning(sa_batch_t b, const int32_t* entries, int n) {
+  if (!b) return fail(SA_ERR_INVALID, "null batch");
+  if (b->finalized) return fail(SA_ERR_INVALID, "set the tuning before finalize");
+  if (n < 0) {
+    b->tuning.clear();
+    b->tuning_set = false;
+    return SA_OK;
+  }
+  if (n > 0 && !entries) return fail(SA_ERR_INVALID, "null tuning entries");
+  b->tuning.assign(n, TuneEntry{});
+  for (int i = 0; i < n; ++i) {
+    const int32_t* e = entries + 7 * i;
+    b->tuning[i] = TuneEntry{e[0], e[1], e[2], e[3], e[4], e[5], e[6]};
+  }
+  b->tuning_set = true;
+  return SA_OK;
+}
+
+int sa_tuning_table(int32_t* out, int cap, int* n) {
+  if (!n) return fail(SA_ERR_INVALID, "null count");
+  const std::vector<TuneEntry>& t = builtin_tuning();
+  *n = (int)t.size();
+  if (!out) return SA_OK;
+  if (cap < (int)t.size()) return fail(SA_ERR_BUFFER, "tuning buffer too small");
+  for (size_t i = 0; i < t.size(); ++i) {
+    const TuneEntry& e = t[i];
+    const int32_t v[7] = {e.lattice, e.L, e.nslots, e.C, e.SL, e.warps, e.hr};
+    memcpy(out + 7 * i, v, sizeof v);
+  }
+  return SA_OK;
+}
+
+int sa_batch_instance_shape(sa_batch_t b, int id, int32_t* out) {
+  if (!b || !out) return fail(SA_ERR_INVALID, "null argument");
+  if (!b->finalized) return fail(SA_ERR_INVALID, "finalize first");
+  if (id < 0 || id >= (int)b->inst.size()) return fail(SA_ERR_INVALID, "no such instance");
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    const sa_batch::Group& g = b->groups[gi];
+    for (int k = g.begin; k < g.begin + g.count; ++k) {
+      if (b->h_order[k] != id) continue;
+      const InstDesc& d = b->inst[id];
+      const int32_t v[7] = {d.lattice, d.L, d.nslots, g.wide ? -1 : (g.resident ? g.C : 0), g.SL, g.threads / 32,
+                            g.hr ? 1 : 0};
+      memcpy(out, v, sizeof v);
+      return SA_OK;
+    }
+  }
+  return fail(SA_ERR_INVALID, "instance not in a launch group");
 }
 
 int sa_batch_launches_per_run(sa_batch_t b, int* n) {
@@ -2309,7 +2432,8 @@ int sa_serve_active(sa_serve_t s, int* n, long long* free_words) {
 namespace sa {
 
 bool resident_ok(const sa_system* sy) {
-  return sy->rng_mode == SA_RNG_PHILOX && sy->h == 0.0 && sy->L >= 4 && sy->N <= kBatchMaxN;
+  return sy->rng_mode == SA_RNG_PHILOX && sy->first_colour == 0 && sy->h == 0.0 && sy->L >= 4 &&
+         sy->N <= kBatchMaxN;
 }
 
 int resident_run(sa_system* sy, const double* T, int nsteps, int sweeps, int stride, int64_t* Emax,

@@ -19,6 +19,14 @@ struct Decision {
   int32_t pair, lo, hi, pad;
 };
 
+// Launch shape of the resident kernel for one bucket of instances
+// (lattice, L, slots): cluster size C, slots per lane SL (lanes per site
+// follow), warps per block, and the high-register form (two-slot 3D only).
+// Chosen per bucket by timing on the GPU (simulated_annealing_b200/autotune.py).
+struct TuneEntry {
+  int32_t lattice, L, nslots, C, SL, warps, hr;
+};
+
 struct InstDesc {
   int32_t lattice, L, nslots, P;   // P: lanes per site group (pow2 >= nslots, <= 32)
   int32_t ladder, sched;           // exactly one >= 0

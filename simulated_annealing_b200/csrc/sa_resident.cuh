@@ -31,6 +31,8 @@ constexpr int kResMaxThreads = kResMaxWarps * 32;
 // the segmented single-slot 3D variant trades threads for registers (its
 // segment maps stay in registers): 16 warps at up to 128 registers
 constexpr int kSegMaxThreads = 512;
+// the high-register form of the two-slot 3D walk: 12 warps, ~170 registers
+constexpr int kHiRegThreads = 384;
 
 struct ResCtx {
   word_t* sm;           // this CTA's rows

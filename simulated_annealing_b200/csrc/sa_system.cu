@@ -228,12 +228,15 @@ __global__ void k_init_J(word_t* __restrict__ J, int L, int dim, long N,
 }
 
 // Counter-based initial spins: block (epoch, 0, i, 2^31 | i>>32), lanes 0,1.
+// tag: 0x80000000, or 0xC0000000 for a system whose first half-sweep is
+// colour 1 (the second configuration of a two-lattice pair draws its initial
+// spins from its own counter range)
 __global__ void k_init_rand(word_t* __restrict__ s, int L, long N, unsigned long long seed,
-                            unsigned long long epoch) {
+                            unsigned long long epoch, uint32_t tag) {
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   uint4x b = philox10((uint32_t)epoch, (uint32_t)(epoch >> 32), (uint32_t)i,
-                      0x80000000u | (uint32_t)((unsigned long long)i >> 32), (uint32_t)seed,
+                      tag | (uint32_t)((unsigned long long)i >> 32), (uint32_t)seed,
                       (uint32_t)(seed >> 32));
   s[split_index(i, L, N / 2, L >> 1)] = (word_t)b.x | ((word_t)b.y << 32);
 }
@@ -548,6 +551,8 @@ int sa_sys_set_seed(sa_system_t sy, uint64_t seed) {
 int sa_sys_set_rng_mode(sa_system_t sy, int mode) {
   if (!sy) return fail(SA_ERR_INVALID, "null system");
   if (mode != SA_RNG_PHILOX && mode != SA_RNG_MT19937_64) return fail(SA_ERR_INVALID, "unknown random mode");
+  if (mode == SA_RNG_MT19937_64 && sy->first_colour != 0)
+    return fail(SA_ERR_UNSUPPORTED, "the mt19937_64 stream has one visiting order: first colour must be 0");
   if (mode == SA_RNG_MT19937_64) {
     ThresholdsMT tm;
     if (!make_thresholds_mt(sy->lattice, sy->T, sy->h, &tm)) return fail(SA_ERR_INVALID, "non-monotone table");
@@ -557,6 +562,21 @@ int sa_sys_set_rng_mode(sa_system_t sy, int mode) {
     return mt_reseed(sy);
   }
   sy->rng_mode = mode;
+  return SA_OK;
+}
+
+int sa_sys_set_first_colour(sa_system_t sy, int colour) {
+  if (!sy) return fail(SA_ERR_INVALID, "null system");
+  if (colour != 0 && colour != 1) return fail(SA_ERR_INVALID, "the first colour is 0 or 1");
+  if (colour != 0 && sy->rng_mode != SA_RNG_PHILOX)
+    return fail(SA_ERR_UNSUPPORTED, "the first colour can be 1 in Philox mode only");
+  sy->first_colour = colour;
+  return SA_OK;
+}
+
+int sa_sys_get_first_colour(sa_system_t sy, int* colour) {
+  if (!sy || !colour) return fail(SA_ERR_INVALID, "null argument");
+  *colour = sy->first_colour;
   return SA_OK;
 }
 
@@ -593,7 +613,8 @@ int sa_sys_init_rand(sa_system_t sy) {
     SA_CUDA_TRY(cudaGetLastError());
     return SA_OK;
   }
-  k_init_rand<<<grid_for(sy->N, 256), 256, 0, sy->stream>>>(sy->d_s, sy->L, sy->N, sy->seed, sy->epoch);
+  k_init_rand<<<grid_for(sy->N, 256), 256, 0, sy->stream>>>(sy->d_s, sy->L, sy->N, sy->seed, sy->epoch,
+                                                              sy->first_colour ? 0xC0000000u : 0x80000000u);
   SA_CUDA_TRY(cudaGetLastError());
   sy->epoch += 1;
   return SA_OK;
@@ -700,9 +721,10 @@ int sa_sys_sweep(sa_system_t sy, long nsweeps) {
     const double T = sy->T;
     return resident_run(sy, &T, 1, (int)nsweeps, 0, nullptr, nullptr, nullptr);
   }
+  const int c0 = sy->first_colour;
   for (long k = 0; k < nsweeps; ++k) {
-    launch_halfsweep(sy, 0, sy->draw);
-    launch_halfsweep(sy, 1, sy->draw + 1);
+    launch_halfsweep(sy, c0, sy->draw);
+    launch_halfsweep(sy, 1 - c0, sy->draw + 1);
     sy->draw += 2;
   }
   SA_CUDA_TRY(cudaGetLastError());
@@ -790,7 +812,7 @@ int sa_sys_device_buffers(sa_system_t sy, uint64_t** d_spins, uint64_t** d_J) {
 // internal spins (N words) and own couplings (dim*N words).
 struct CkptHeader {
   char magic[8];
-  int32_t version, lattice, L, pad;
+  int32_t version, lattice, L, pad;  // pad: the first colour
   double T, h;
   uint64_t seed, draw, epoch;
 };
@@ -806,6 +828,7 @@ int sa_sys_save(sa_system_t sy, void* buf, size_t cap, size_t* len) {
   memset(&hd, 0, sizeof hd);
   memcpy(hd.magic, "SAB200CK", 8);
   hd.version = mt_bytes ? 2 : 1;  // 2: mt19937_64 mode, generator state appended
+  hd.pad = sy->first_colour;      // 0 in records written before the field existed
   hd.lattice = sy->lattice;
   hd.L = sy->L;
   hd.T = sy->T;
@@ -862,6 +885,7 @@ int sa_sys_load(sa_system_t sy, const void* buf, size_t len) {
   sy->seed = hd.seed;
   sy->draw = hd.draw;
   sy->epoch = hd.epoch;
+  sy->first_colour = (hd.pad == 1 && !mt) ? 1 : 0;
   return SA_OK;
 }
 

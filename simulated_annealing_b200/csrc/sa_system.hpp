@@ -21,6 +21,11 @@ struct sa_system {
   // draw counter above) or SA_RNG_MT19937_64 (the CPU reference's stream; its
   // state lives on the device in d_mt, the pass's outputs in d_draws).
   int rng_mode = 0;
+  // Colour of the first half-sweep of every sweep (draw t+2n; the other
+  // colour takes t+2n+1). 1 is the second configuration of the reference GPU
+  // systems' two-lattice pair (src/gpu_2d.cu:109-120): its odd sites are
+  // updated first. Philox mode only.
+  int first_colour = 0;
   uint64_t* d_mt = nullptr;        // [kMtN + 1]: state words, next index
   uint64_t* d_draws = nullptr;     // dim * N outputs (init_J is the largest pass)
   sa::ThresholdsMT thr_mt{};

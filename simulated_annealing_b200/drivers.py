@@ -124,15 +124,18 @@ class ParallelTempering:
                 e0 = self.E[0]
                 self.E_min = e0.copy() if self.E_min.size == 0 else np.maximum(self.E_min, e0)
         i, r = self._next_pair()
-        Ei = np.ascontiguousarray(self.E[i], dtype=np.float32)
-        Ej = np.ascontiguousarray(self.E[i + 1], dtype=np.float32)
-        mask = int(self._lib.sa_pt_mask(Ei.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
-                                        Ej.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
-                                        self.T[i], self.T[i + 1], r))
-        self.acc_sum[i] += bin(mask).count("1") / 64.0
+        # one mask word per 64 replicas (src/parallel_tempering.hpp:143-160)
+        masks = []
+        for w in range(len(self.E[i]) // 64):
+            Ei = np.ascontiguousarray(self.E[i][64 * w:64 * w + 64], dtype=np.float32)
+            Ej = np.ascontiguousarray(self.E[i + 1][64 * w:64 * w + 64], dtype=np.float32)
+            masks.append(int(self._lib.sa_pt_mask(Ei.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                  Ej.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                  self.T[i], self.T[i + 1], r)))
+        self.acc_sum[i] += sum(bin(m).count("1") for m in masks) / 64.0
         self.acc_n[i] += 1
-        self.sys[i].swap(self.sys[i + 1], mask)
-        return i, mask
+        self.sys[i].swap(self.sys[i + 1], masks if len(masks) > 1 else masks[0])
+        return i, (masks if len(masks) > 1 else masks[0])
 
     def acceptance(self) -> np.ndarray:
         """accumulator<double>::get() per pair: the mean accepted fraction."""
@@ -199,20 +202,11 @@ class ParallelTempering:
 
     @staticmethod
     def _record(s) -> bytes:
-        if s.rng_mode() == _lib.SA_RNG_MT19937_64:
-            return s.save_reference()
-        blob = s.save()
-        return struct.pack("<Q", len(blob)) + blob
+        return s.checkpoint_record()
 
     @staticmethod
     def _read_record(s, data: bytes, off: int) -> int:
-        if s.rng_mode() == _lib.SA_RNG_MT19937_64:
-            n = len(s.save_reference())
-            s.load_reference(data[off:off + n])
-            return off + n
-        (n,) = struct.unpack_from("<Q", data, off)
-        s.load(data[off + 8:off + 8 + n])
-        return off + 8 + n
+        return s.read_checkpoint_record(data, off)
 
     def save(self) -> bytes:
         out = [struct.pack("<q??", self.steps, self.print_E, self.print_min), self._gen_bytes()]

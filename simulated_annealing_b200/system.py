@@ -104,6 +104,17 @@ class GpuSystem:
             mode = {"philox": _lib.SA_RNG_PHILOX, "mt19937_64": _lib.SA_RNG_MT19937_64}[mode]
         check(self._lib.sa_sys_set_rng_mode(self._h, int(mode)))
 
+    def set_first_colour(self, colour: int) -> None:
+        """Colour of each sweep's first half-sweep (sa_sys_set_first_colour):
+        1 is the second configuration of the reference GPU systems'
+        two-lattice pair. Philox mode only."""
+        check(self._lib.sa_sys_set_first_colour(self._h, int(colour)))
+
+    def first_colour(self) -> int:
+        c = ctypes.c_int()
+        check(self._lib.sa_sys_get_first_colour(self._h, ctypes.byref(c)))
+        return c.value
+
     def rng_mode(self) -> int:
         m = ctypes.c_int()
         check(self._lib.sa_sys_get_rng_mode(self._h, ctypes.byref(m)))
@@ -171,15 +182,40 @@ class GpuSystem:
         check(self._lib.sa_sys_load(self._h, buf, len(data)))
 
     def clone(self) -> "GpuSystem":
-        """A copy of this system (cpu_sys::clone, src/cpu_sys.hpp:30): same
-        lattice, temperature, field, random mode and position, spins and
-        couplings, in a new device allocation."""
+        """A copy of this system (cpu_sys::clone, src/cpu_sys.hpp:30) in a new
+        device allocation: same lattice, temperature, field, spins and
+        couplings. In mt19937_64 mode the copy's generator is reseeded with
+        1234, as the reference's copy constructors do (src/cpu_3d.cpp:47-78,
+        src/cpu_2dp.cpp:53-84); in Philox mode it keeps the seed and position.
+        (The reference's cpu_2d inherits cpu_2dp::clone and so copies a
+        periodic lattice into an open-x one; here the lattice is kept.)"""
         c = GpuSystem(self.lattice, self.L, self.get_T(), self.h)
         if self.rng_mode() == _lib.SA_RNG_MT19937_64:
             c.load_reference(self.save_reference())
+            c.set_seed(1234)
         else:
             c.load(self.save())
         return c
+
+    def checkpoint_record(self) -> bytes:
+        """The system's part of a parallel-tempering checkpoint: in
+        mt19937_64 mode the reference CPU classes' own record (cpu_2dp::save /
+        cpu_3d::save), else this engine's record with an 8-byte length in
+        front (what the C++ gpu_sys shim writes)."""
+        if self.rng_mode() == _lib.SA_RNG_MT19937_64:
+            return self.save_reference()
+        blob = self.save()
+        return struct.pack("<Q", len(blob)) + blob
+
+    def read_checkpoint_record(self, data: bytes, off: int) -> int:
+        """Loads checkpoint_record()'s bytes at data[off:]; returns the end."""
+        if self.rng_mode() == _lib.SA_RNG_MT19937_64:
+            n = len(self.save_reference())
+            self.load_reference(data[off:off + n])
+            return off + n
+        (n,) = struct.unpack_from("<Q", data, off)
+        self.load(data[off + 8:off + 8 + n])
+        return off + 8 + n
 
     def save_reference(self) -> bytes:
         """The record cpu_2dp::save / cpu_3d::save write (mt19937_64 mode)."""
@@ -247,3 +283,95 @@ class GpuSystem:
             self.gpu_free()
         except Exception:
             pass
+
+
+class TwoLatticeSystem:
+    """The reference GPU systems' own shape (gpu_2d, gpu_3d): 128 replicas per
+    system. Their two lattices s1, s2, each updated from the other
+    (src/gpu_2d.cu:109-120), carry two configurations: A (s1 on colour-0
+    sites, s2 on colour-1 sites), whose sweep updates colour 0 first, and B,
+    which updates colour 1 first. Here they are two GpuSystem objects with the
+    same couplings, B with first colour 1. measure() returns A's 64 values
+    then B's (src/gpu_2d.cu:196-205); swap() takes two mask words
+    (src/parallel_tempering.hpp:143-149). Philox mode only."""
+
+    def __init__(self, lattice, L: int, T: float = 1.0, h: float = 0.0):
+        self.a = GpuSystem(lattice, L, T, h)
+        self.b = GpuSystem(lattice, L, T, h)
+        self.b.set_first_colour(1)
+        self.lattice, self.L, self.N, self.h = self.a.lattice, self.a.L, self.a.N, self.a.h
+
+    def _both(self, name, *args):
+        for s in (self.a, self.b):
+            getattr(s, name)(*args)
+
+    def sweep(self, n: int = 1) -> None:
+        self._both("sweep", n)
+
+    def set_T(self, T: float) -> None:
+        self._both("set_T", T)
+
+    def get_T(self) -> float:
+        return self.a.get_T()
+
+    def set_h(self, h: float) -> None:
+        self._both("set_h", h)
+        self.h = float(h)
+
+    def set_seed(self, seed: int) -> None:
+        self._both("set_seed", seed)
+
+    def init_J(self) -> None:
+        self._both("init_J")
+
+    def init_rand(self) -> None:
+        self._both("init_rand")
+
+    def rng_mode(self) -> int:
+        return _lib.SA_RNG_PHILOX
+
+    def measure(self) -> list[float]:
+        return self.a.measure() + self.b.measure()
+
+    def get_N(self) -> int:
+        return self.N
+
+    def swap(self, other: "TwoLatticeSystem", mask) -> None:
+        m = list(mask) if hasattr(mask, "__len__") else [int(mask), 0]
+        self.a.swap(other.a, int(m[0]))
+        self.b.swap(other.b, int(m[1]))
+
+    def load_J(self, fname: str) -> None:
+        self._both("load_J", fname)
+
+    def save_J(self, fname: str) -> None:
+        self.a.save_J(fname)
+
+    def get_J(self):
+        return self.a.get_J()
+
+    def save(self) -> bytes:
+        ra, rb = self.a.save(), self.b.save()
+        return struct.pack("<Q", len(ra)) + ra + struct.pack("<Q", len(rb)) + rb
+
+    def load(self, data: bytes) -> None:
+        (n,) = struct.unpack_from("<Q", data, 0)
+        self.a.load(data[8:8 + n])
+        (m,) = struct.unpack_from("<Q", data, 8 + n)
+        self.b.load(data[16 + n:16 + n + m])
+
+    def checkpoint_record(self) -> bytes:
+        """A's record then B's, each with its length (the C++ shim's layout)."""
+        return self.a.checkpoint_record() + self.b.checkpoint_record()
+
+    def read_checkpoint_record(self, data: bytes, off: int) -> int:
+        off = self.a.read_checkpoint_record(data, off)
+        return self.b.read_checkpoint_record(data, off)
+
+    def clone(self) -> "TwoLatticeSystem":
+        c = TwoLatticeSystem(self.lattice, self.L, self.get_T(), self.h)
+        c.load(self.save())
+        return c
+
+    def gpu_free(self) -> None:
+        self._both("gpu_free")

@@ -1,0 +1,104 @@
+"""The tuned launch shapes of the batched engine.
+
+simulated_annealing_b200/autotune.py times candidate shapes per bucket on the
+GPU and writes the winners into the table compiled into the library
+(csrc/sa_tuning.inc, record in tuning.json). Every tuned shape must keep the
+engine bit-exact: one instance of each bucket runs in exactly that shape
+(checked through sa_batch_instance_shape) against the oracle's
+parallel_tempering<>.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+ROOT = os.path.dirname(HERE)
+JSON = os.path.join(ROOT, "simulated_annealing_b200", "tuning.json")
+INC = os.path.join(ROOT, "simulated_annealing_b200", "csrc", "sa_tuning.inc")
+
+
+def _inc_rows():
+    rows = []
+    for ln in open(INC):
+        ln = ln.strip()
+        if ln.startswith("{"):
+            rows.append([int(v) for v in ln.strip("{},").split(",")])
+    return rows
+
+
+def test_table_and_record_agree():
+    rows = _inc_rows()
+    for r in rows:
+        assert len(r) == 7 and r[0] in (0, 1, 2) and r[1] % 2 == 0 and r[3] >= 1 and r[4] in (1, 2)
+    if os.path.exists(JSON):
+        rec = json.load(open(JSON))
+        assert [list(map(int, e)) for e in rec["table"]] == rows
+        for b in rec["buckets"]:
+            if b["best"] is not None:
+                assert b["best_rate"] > b["heuristic_rate"]
+
+
+@pytest.mark.gpu
+def test_every_tuned_shape_is_bit_exact(sab):
+    from simulated_annealing_b200.batch import Batch, tuning_table
+    from test_gpu_batch import check_instance
+
+    table = tuning_table()
+    assert table.tolist() == _inc_rows()
+    for row in table:
+        lat, L, nslots = (int(v) for v in row[:3])
+        T = list(np.geomspace(0.5, 2.0, nslots) if lat == O.LAT_3D else np.geomspace(0.3, 1.6, nslots))
+        b = Batch()
+        lad = b.add_ladder(T)
+        b.add_instance(lat, L, ladder=lad, seed_J=70 + L, seed=71 + L)
+        b.set_spread(False)
+        b.finalize()
+        assert b.shape(0) == tuple(int(v) for v in row), row
+        b.record_exchanges(16)
+        b.run(5)
+        b.run(4)
+        b.sync()
+        check_instance(b, 0, lat, L, T, 70 + L, 71 + L, 9)
+        b.close()
+
+
+@pytest.mark.gpu
+def test_explicit_shapes_and_fallback(sab):
+    """A shape given through sa_batch_set_tuning is used (two-slot high-register
+    3D walk on a larger cluster); an unusable one (odd slots with SL = 2)
+    falls back to the heuristic shape; both stay bit-exact."""
+    from simulated_annealing_b200.batch import Batch
+    from test_gpu_batch import check_instance
+
+    T = list(np.geomspace(0.5, 2.0, 6))
+    b = Batch()
+    lad = b.add_ladder(T)
+    b.add_instance(O.LAT_3D, 10, ladder=lad, seed_J=5, seed=6)
+    b.set_tuning([[O.LAT_3D, 10, 6, 2, 2, 5, 1]])
+    b.set_spread(False)
+    b.finalize()
+    assert b.shape(0) == (O.LAT_3D, 10, 6, 2, 2, 5, 1)
+    b.record_exchanges(8)
+    b.run(7)
+    b.sync()
+    check_instance(b, 0, O.LAT_3D, 10, T, 5, 6, 7)
+    b.close()
+    T5 = list(np.geomspace(0.5, 2.0, 5))
+    b = Batch()
+    lad = b.add_ladder(T5)
+    b.add_instance(O.LAT_3D, 10, ladder=lad, seed_J=5, seed=6)
+    b.set_tuning([[O.LAT_3D, 10, 5, 2, 2, 5, 1]])
+    b.set_spread(False)
+    b.finalize()
+    assert b.shape(0)[4] == 1
+    b.record_exchanges(8)
+    b.run(7)
+    b.sync()
+    check_instance(b, 0, O.LAT_3D, 10, T5, 5, 6, 7)
+    b.close()
