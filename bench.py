@@ -372,12 +372,14 @@ def c4_config(args, world: int) -> dict:
             "parallelism": f"instances sharded, {world} GPU(s), no collective"}
 
 
-def build_c4_batch(insts, stream_ptr=None):
+def build_c4_batch(insts, stream_ptr=None, group_timing=False):
     """The batched mix as the bench runs it: one batch, the two 16-slot
     ladders, the instances in order (tests build the same batch)."""
     from simulated_annealing_b200.batch import Batch
 
     b = Batch()
+    if group_timing:
+        b.set_group_timing(True)
     l2 = b.add_ladder(LADDER_2D)
     l3 = b.add_ladder(LADDER_3D)
     for lat, L, seed in insts:
@@ -438,7 +440,7 @@ def run_ours(args):
 
     insts = shard_instances(rank, world, args.instances)
     stream = torch.cuda.Stream()
-    b = build_c4_batch(insts, stream.cuda_stream)
+    b = build_c4_batch(insts, stream.cuda_stream, group_timing=True)
     S = args.sweeps_per_step
     site_slots = b.site_slots()
     attempts_step = site_slots * 64 * S
@@ -465,6 +467,10 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     barrier()
+
+    # the end of every shape group in the last timed step (one stream per
+    # group; the step ends with the slowest)
+    groups = b.group_times()
 
     # e2e through the public API with host buffers (pinned)
     E_host = torch.empty(b.energy_count(), dtype=torch.int64, pin_memory=True)
@@ -512,6 +518,7 @@ def run_ours(args):
                                  "(spins in and out once, couplings once) is far below the algorithmic bytes; "
                                  "the kernel is bound by integer-ALU issue"},
             "clocks": clk,
+            "groups_last_step": groups,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_sample(insts, args.cpu_budget)

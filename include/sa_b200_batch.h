@@ -87,6 +87,14 @@ int sa_tuning_table(int32_t* out, int cap, int* n);
 int sa_batch_set_tuning(sa_batch_t b, const int32_t* entries, int n);
 int sa_batch_set_spread(sa_batch_t b, int on);
 int sa_batch_instance_shape(sa_batch_t b, int id, int32_t* out);
+/* Per launch group (one shape per group, each on its own stream): with
+ * sa_batch_set_group_timing(b, 1) before finalize, sa_batch_group_times
+ * gives, for the last sa_batch_run, each group's five int32 (lattice, L,
+ * instances, C, warps) and the milliseconds from the run's start to the
+ * group's end -- the tail of the slowest group. info / ms may be NULL;
+ * *n receives the group count. No counterpart in the reference. */
+int sa_batch_set_group_timing(sa_batch_t b, int on);
+int sa_batch_group_times(sa_batch_t b, int32_t* info, float* ms, int cap, int* n);
 /* Sweeps between exchange attempts (the PT template's `steps`; default 1). */
 int sa_batch_set_exchange_interval(sa_batch_t b, int sweeps_per_exchange);
 /* Anneal instances: measure every `stride` sweeps (0 = never; default 1) and

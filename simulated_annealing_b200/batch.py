@@ -59,6 +59,8 @@ for _name, _res, _args in [
     ("sa_batch_set_tuning", _c.c_int, [_vp, _c.POINTER(_c.c_int32), _c.c_int]),
     ("sa_batch_set_spread", _c.c_int, [_vp, _c.c_int]),
     ("sa_batch_instance_shape", _c.c_int, [_vp, _c.c_int, _c.POINTER(_c.c_int32)]),
+    ("sa_batch_set_group_timing", _c.c_int, [_vp, _c.c_int]),
+    ("sa_batch_group_times", _c.c_int, [_vp, _c.POINTER(_c.c_int32), _c.POINTER(_c.c_float), _c.c_int, _ip]),
 ]:
     _lib.register(_name, _res, _args)
 
@@ -125,6 +127,21 @@ class Batch:
             return
         a = np.ascontiguousarray(np.asarray(entries, dtype=np.int32).reshape(-1, 7))
         check(self._lib.sa_batch_set_tuning(self._h, _p(a, _c.c_int32), len(a)))
+
+    def set_group_timing(self, on: bool) -> None:
+        check(self._lib.sa_batch_set_group_timing(self._h, int(bool(on))))
+
+    def group_times(self):
+        """Per launch group of the last run: dicts of lattice, L, instances,
+        C, warps and the ms from the run's start to the group's end."""
+        n = _c.c_int()
+        check(self._lib.sa_batch_group_times(self._h, None, None, 0, _c.byref(n)))
+        info = np.zeros((max(n.value, 1), 5), dtype=np.int32)
+        ms = np.zeros(max(n.value, 1), dtype=np.float32)
+        check(self._lib.sa_batch_group_times(self._h, _p(info, _c.c_int32), _p(ms, _c.c_float), n.value,
+                                             _c.byref(n)))
+        return [{"lattice": int(r[0]), "L": int(r[1]), "instances": int(r[2]), "C": int(r[3]), "warps": int(r[4]),
+                 "end_ms": round(float(t), 3)} for r, t in zip(info[: n.value], ms[: n.value])]
 
     def set_spread(self, on: bool) -> None:
         check(self._lib.sa_batch_set_spread(self._h, int(bool(on))))

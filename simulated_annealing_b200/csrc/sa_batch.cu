@@ -835,6 +835,7 @@ struct sa_batch {
   bool force_global = false;   // run every instance in the global-memory kernel
   bool no_wide = false;        // never run an instance wide (sa_wide.cuh)
   bool no_spread = false;      // keep full-batch launch shapes even when SMs sit idle
+  bool group_timing = false;   // fork / done events with timing (sa_batch_group_times)
   std::vector<TuneEntry> tuning;  // launch shapes per bucket (empty: the built-in table)
   bool tuning_set = false;
   int hstride = 0;             // energy histograms every hstride sweeps (0 = off)
@@ -1656,11 +1657,12 @@ int sa_batch_finalize(sa_batch_t b) {
   b->h_xsteps.assign(ni, 0);
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-  SA_CUDA_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+  const unsigned ev_flags = b->group_timing ? cudaEventDefault : cudaEventDisableTiming;
+  SA_CUDA_TRY(cudaEventCreateWithFlags(&b->fork, ev_flags));
   for (size_t gi = 0; gi < b->groups.size(); ++gi) {
     sa_batch::Group& g = b->groups[gi];
     SA_CUDA_TRY(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
-    SA_CUDA_TRY(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+    SA_CUDA_TRY(cudaEventCreateWithFlags(&g.done, ev_flags));
     if (g.resident) {
       int mc = 0;
       int st = dispatch(b, g, (int)gi, 0, 1, &mc);
@@ -1711,6 +1713,33 @@ int sa_batch_set_kernel(sa_batch_t b, int kernel) {
   if (b->finalized) return fail(SA_ERR_INVALID, "choose the kernel before finalize");
   b->force_global = (kernel == 1);
   b->no_wide = (kernel == 2);
+  return SA_OK;
+}
+
+int sa_batch_set_group_timing(sa_batch_t b, int on) {
+  if (!b) return fail(SA_ERR_INVALID, "null batch");
+  if (b->finalized) return fail(SA_ERR_INVALID, "set group timing before finalize");
+  b->group_timing = on != 0;
+  return SA_OK;
+}
+
+int sa_batch_group_times(sa_batch_t b, int32_t* info, float* ms, int cap, int* n) {
+  if (!b || !n) return fail(SA_ERR_INVALID, "null argument");
+  if (!b->finalized || !b->group_timing) return fail(SA_ERR_INVALID, "enable group timing before finalize");
+  *n = (int)b->groups.size();
+  if (!info && !ms) return SA_OK;
+  if (cap < *n) return fail(SA_ERR_BUFFER, "group buffer too small");
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    const sa_batch::Group& g = b->groups[gi];
+    if (info) {
+      const int32_t v[5] = {g.lattice, g.L, g.count, g.wide ? -1 : (g.resident ? g.C : 0), g.threads / 32};
+      memcpy(info + 5 * gi, v, sizeof v);
+    }
+    if (ms) {
+      SA_CUDA_TRY(cudaEventSynchronize(g.done));
+      SA_CUDA_TRY(cudaEventElapsedTime(&ms[gi], b->fork, g.done));
+    }
+  }
   return SA_OK;
 }
 

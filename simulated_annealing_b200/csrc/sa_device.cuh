@@ -207,10 +207,13 @@ struct VCount {
       }
     }
   }
-  __device__ __forceinline__ unsigned count_of(int j) const {
+  __device__ __forceinline__ unsigned count_of(int j) const { return count_low<B>(j); }
+  // the count of replica j from the low NB planes (the others known zero)
+  template <int NB>
+  __device__ __forceinline__ unsigned count_low(int j) const {
     unsigned v = 0;
 #pragma unroll
-    for (int b = 0; b < B; ++b) v |= (unsigned)((p[b] >> j) & 1ULL) << b;
+    for (int b = 0; b < NB && b < B; ++b) v |= (unsigned)((p[b] >> j) & 1ULL) << b;
     return v;
   }
 };

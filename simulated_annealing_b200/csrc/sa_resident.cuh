@@ -335,6 +335,10 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
     SlotWords<SL> prev = {};
     if (valid) prev = ldw<SL>(x.sm + own + (L - 1) * zs);
     SlotWords<SL> first = {};
+    // the plane's own words: plane 0's loaded here, every later plane's as
+    // the z+1 neighbour of the plane below (only this lane writes them)
+    SlotWords<SL> cur = {};
+    if (valid) cur = ldw<SL>(x.sm + own);
     word_t jnext = __ldg(Jzc + jo);  // the z-1 coupling of the next plane (plane 0: the wrapped bond)
     // A warp whose lanes all have a site and a slot (every warp of the
     // batched ensembles) walks without the per-lane test.
@@ -358,10 +362,12 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         bs = __ldg(Jyo + js + zo);
         bd = __ldg(Jzc + jo + ((zd == L - 1) ? 0 : zo + zg));
       }
-#pragma unroll 4
-      for (int zi = 0; zi < P; ++zi) {
-        const int z = z0 + zi;
-        if (z >= L) break;  // warp-uniform
+      // One plane. POS 1: plane 0 (its new words are the top plane's z+1
+      // neighbours); 2: plane L-1 (its z+1 neighbour is the new plane 0);
+      // 0: any other. The position is known where the step is placed, so a
+      // step carries no test of z.
+      auto step = [&](int zi, auto pos) {
+        constexpr int POS = decltype(pos)::value;
         const int src = cl * P + zi;
         // one lane per site (P = 1): the lane's own draw and couplings
         const uint32_t u = (P == 1) ? um : __shfl_sync(0xffffffffu, um, src);
@@ -373,9 +379,8 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
         const word_t jd = (P == 1) ? bd : __shfl_sync(0xffffffffu, bd, src);
         jnext = jd;
         if (!CHECK || valid) {
-          const bool last = (z == L - 1);
-          const SlotWords<SL> si = ldw<SL>(x.sm + own);
-          const SlotWords<SL> sd = last ? first : ldw<SL>(x.sm + own + zs);
+          const SlotWords<SL> si = cur;
+          const SlotWords<SL> sd = (POS == 2) ? first : ldw<SL>(x.sm + own + zs);
           const SlotWords<SL> sw = ldw<SL>(x.sm + ow);
           const SlotWords<SL> se = ldw<SL>(x.sm + oe);
           const SlotWords<SL> sn = pn.template ld<SL>(0);
@@ -391,15 +396,27 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
             nsw.w[q] = flip_below(si.w[q], c0, c1, c2, m0, m1, m2);
           }
           stw<SL>(x.sm + own, nsw);
-          if (z == 0) first = nsw;
+          if (POS == 1) first = nsw;
           prev = nsw;
+          cur = sd;
         }
         own += zs;
         ow += zs;
         oe += zs;
         pn.step(zsn);
         ps.step(zss);
+      };
+      const int nz = min(P, L - z0);             // planes in this block (warp-uniform)
+      const bool top = (z0 + nz == L);           // the block holds plane L-1
+      int zi = 0;
+      if (z0 == 0) {
+        step(0, std::integral_constant<int, 1>{});
+        zi = 1;
       }
+      const int zend = top ? nz - 1 : nz;
+#pragma unroll 4
+      for (; zi < zend; ++zi) step(zi, std::integral_constant<int, 0>{});
+      if (top) step(nz - 1, std::integral_constant<int, 2>{});
     }
     };
     if (__all_sync(0xffffffffu, valid)) walk(std::false_type{});
@@ -887,10 +904,12 @@ __device__ __forceinline__ void rmeasure_body(const ResCtx& x, bool d3, bool ope
     }
     add_small_w<W0>(big, sm4);
     warp_sum_grow<NSL, W0>(big);
+    // planes the sum can reach: W0 per lane, one more per butterfly level
+    constexpr int NBU = W0 + ((NSL == 1) ? 5 : (NSL == 2) ? 4 : 3);
 #pragma unroll
     for (int m = 0; m < 2 * NSL; ++m) {
       const int j = (lane / NSL) + per * m;
-      atomicAdd(&cnt[q][j], big.count_of(j));
+      atomicAdd(&cnt[q][j], big.template count_low<NBU>(j));
     }
   }
 }

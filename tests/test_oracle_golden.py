@@ -83,3 +83,11 @@ def test_philox_bulk_matches_curand(oracle):
                             f.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
         assert hashlib.sha256(u.tobytes()).hexdigest() == h["u32_sha256"], seed
         assert hashlib.sha256(f.tobytes()).hexdigest() == h["uniform_bits_sha256"], seed
+
+
+def test_uniform_is_monotone_over_every_u32(oracle):
+    """Exhaustive over all 2^32 inputs: the u32 -> uniform map (pinned to
+    curand_uniform above) is non-decreasing, lies in (0, 1] and reaches 1.
+    With it, "uniform(u) < b" is "u < thr(b)" for every u, which is what the
+    engine's integer thresholds compute."""
+    assert oracle.oracle_lib().sao_check_uniform_monotone() == 0
