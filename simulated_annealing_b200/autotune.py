@@ -34,6 +34,10 @@ LADDER_3D = np.geomspace(0.5, 2.0, 16)
 # the batched mix's buckets (16 slots) and the 32-temperature ensemble
 BUCKETS = [(LAT_2D, L, 16) for L in (16, 24, 32, 48, 64)] + [(LAT_3D, L, 16) for L in (8, 12, 16, 20, 24)] + \
           [(LAT_3D, 16, 32)]
+# single-slot anneals (the serving requests: every even size they come in,
+# -H measured after every sweep), timed as full batches of that size
+SERVE_BUCKETS = [(LAT_3D, L, 1) for L in range(8, 65, 2)] + [(LAT_2D, L, 1) for L in range(16, 129, 2)]
+SERVE_SITES = 2_500_000  # sites per single-slot batch (~20 MB of spins)
 
 
 def resident_bytes(lat, L, nslots, C):
@@ -57,7 +61,9 @@ def candidates(lat, L, nslots):
                 rp <<= 1
             his = [0, 1] if (SL == 2 and lat == LAT_3D) else [0]
             for hr in his:
-                cap = 12 if hr else 20
+                # the engine's caps: 12 warps for the high-register form, 16 for
+                # single-slot 3D (its walk keeps more words live), else 20
+                cap = 12 if hr else (16 if (lat == LAT_3D and SL == 1 and rp == 1) else 20)
                 # 3D: one lane group of rp lanes per column; 2D: warps take
                 # tiles of 32 sites (the rp lanes of a site inside a tile)
                 passes = max(1, -(-(cols * rp) // 32)) if lat == LAT_3D else max(1, -(-cols // 32))
@@ -76,9 +82,14 @@ def time_shape(lat, L, nslots, n, tuning, sweeps, stream):
     from simulated_annealing_b200.batch import Batch
 
     b = Batch()
-    lad = b.add_ladder(np.geomspace(0.5, 2.0, nslots) if lat == LAT_3D else np.geomspace(0.3, 1.6, nslots))
-    for k in range(n):
-        b.add_instance(lat, L, ladder=lad, seed_J=1000 + k, seed=1000 + k)
+    if nslots == 1:
+        sch = b.add_schedule(np.linspace(3.0, 0.2, 1000), 100)
+        for k in range(n):
+            b.add_instance(lat, L, schedule=sch, seed_J=1000 + k, seed=1000 + k)
+    else:
+        lad = b.add_ladder(np.geomspace(0.5, 2.0, nslots) if lat == LAT_3D else np.geomspace(0.3, 1.6, nslots))
+        for k in range(n):
+            b.add_instance(lat, L, ladder=lad, seed_J=1000 + k, seed=1000 + k)
     b.set_tuning(tuning)
     b.set_spread(False)
     b.finalize()
@@ -107,18 +118,27 @@ def main():
     ap.add_argument("--instances", type=int, default=410, help="instances per bucket (a full GPU)")
     ap.add_argument("--sweeps", type=int, default=40)
     ap.add_argument("--margin", type=float, default=0.01, help="keep a shape only if this much faster")
+    ap.add_argument("--buckets", choices=["mix", "serve", "all"], default="all")
+    ap.add_argument("--keep", default=None, help="a JSON record whose table entries for other buckets are kept")
     args = ap.parse_args()
     stream = torch.cuda.Stream()
     record = {"device": torch.cuda.get_device_name(0), "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
               "instances": args.instances, "sweeps": args.sweeps, "buckets": []}
     table = []
-    for lat, L, nslots in BUCKETS:
-        base, base_shape = time_shape(lat, L, nslots, args.instances, [], args.sweeps, stream)
+    buckets = {"mix": BUCKETS, "serve": SERVE_BUCKETS, "all": BUCKETS + SERVE_BUCKETS}[args.buckets]
+    if args.keep:
+        old = json.load(open(args.keep))
+        mine = {tuple(b) for b in buckets}
+        table = [e for e in old["table"] if tuple(e[:3]) not in mine]
+        record["buckets"] = [b for b in old["buckets"] if tuple(b["bucket"]) not in mine]
+    for lat, L, nslots in buckets:
+        n = args.instances if nslots > 1 else max(8, SERVE_SITES // (L ** 3 if lat == LAT_3D else L * L))
+        base, base_shape = time_shape(lat, L, nslots, n, [], args.sweeps, stream)
         best, best_rate = None, base
         tried = []
         for cand in candidates(lat, L, nslots):
             try:
-                rate, shape = time_shape(lat, L, nslots, args.instances, [list(cand)], args.sweeps, stream)
+                rate, shape = time_shape(lat, L, nslots, n, [list(cand)], args.sweeps, stream)
             except Exception as e:  # a shape the GPU cannot schedule
                 tried.append({"shape": list(cand), "error": str(e)[:120]})
                 continue
@@ -132,12 +152,12 @@ def main():
             table.append(best)
         print(json.dumps(record["buckets"][-1]["bucket"]), "heuristic", round(base, 1), "best", best,
               round(best_rate, 1), flush=True)
-    record["table"] = table
+    record["table"] = sorted(table)
     if args.json:
         with open(args.json, "w") as f:
             json.dump(record, f, indent=1)
     if args.inc:
-        write_inc(args.inc, table, record)
+        write_inc(args.inc, record["table"], record)
 
 
 def write_inc(path, table, record):

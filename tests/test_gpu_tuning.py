@@ -53,6 +53,9 @@ def test_every_tuned_shape_is_bit_exact(sab):
     assert table.tolist() == _inc_rows()
     for row in table:
         lat, L, nslots = (int(v) for v in row[:3])
+        if nslots == 1:
+            _check_single_slot(row)
+            continue
         T = list(np.geomspace(0.5, 2.0, nslots) if lat == O.LAT_3D else np.geomspace(0.3, 1.6, nslots))
         b = Batch()
         lad = b.add_ladder(T)
@@ -66,6 +69,36 @@ def test_every_tuned_shape_is_bit_exact(sab):
         b.sync()
         check_instance(b, 0, lat, L, T, 70 + L, 71 + L, 9)
         b.close()
+
+
+def _check_single_slot(row):
+    """A single-slot anneal (a serving request's shape) in its tuned shape,
+    two instances, against the oracle's annealing<> restatement."""
+    from simulated_annealing_b200.batch import Batch
+
+    lat, L = int(row[0]), int(row[1])
+    Ts = [2.5, 1.6, 0.7]  # linear, as the oracle's anneal(2.5, 1, 0.7, 3, ...) steps
+    b = Batch()
+    sch = b.add_schedule(Ts, 2)
+    for k in range(2):
+        b.add_instance(lat, L, schedule=sch, seed_J=80 + k, seed=90 + k)
+    b.set_spread(False)
+    b.finalize()
+    assert b.shape(0) == tuple(int(v) for v in row), row
+    b.run(6)
+    b.sync()
+    for k in range(2):
+        o = O.OracleSystem(lat, L, mode=O.MODE_PHILOX)
+        o.set_seed(80 + k)
+        o.init_J()
+        o.set_seed(90 + k)
+        o.init_rand()
+        mn, _ = o.anneal(2.5, 1, 0.7, 3, 2, 1)
+        E, done = b.anneal_result(k)
+        assert done == 6
+        assert np.array_equal(E.astype(np.float32), mn), (row, k)
+        assert np.array_equal(b.spins(k, 0), o.spins()), (row, k)
+    b.close()
 
 
 @pytest.mark.gpu
