@@ -136,6 +136,19 @@ int sa_sys_get_rng_mode(sa_system_t sys, int* mode);
  * spins from a counter range of its own. Philox mode only. */
 int sa_sys_set_first_colour(sa_system_t sys, int colour);
 int sa_sys_get_first_colour(sa_system_t sys, int* colour);
+/* The reference's SPLIT_H update (src/device_2d.cu:27-50,
+ * src/device_3d.cu:216-245, tables src/gpu_2d.cu:133-139,
+ * src/gpu_3d.cu:57-63), off by default as in the reference's build: a flip is
+ * accepted in two parts, each site drawing two uniforms per half-sweep (draw
+ * t+2m for the bonds, t+2m+1 for the field). The bond part for n satisfied of
+ * z bonds is accepted always when 2n <= z, else iff u1 < float(exp(-2j/T)),
+ * j = 2n - z (open-x border sites count their forced bond: j = 2n - 5); an up
+ * spin's field part iff u2 < float(exp(-2h/T)) (not clamped), a down spin's
+ * always. In 3D a site with a coordinate 0 or L-1 uses its field draw for the
+ * bond part too, as the reference's boundary branch does. Philox mode only;
+ * sweeps run two launches per sweep. */
+int sa_sys_set_split_field(sa_system_t sys, int on);
+int sa_sys_get_split_field(sa_system_t sys, int* on);
 /* The reference CPU classes' own checkpoint record, byte for byte as
  * cpu_2dp::save / cpu_3d::save write it (src/cpu_2dp.cpp:444-456,
  * src/cpu_3d.cpp:449-461): L, T, h, spins, the reference-layout couplings and

@@ -77,6 +77,7 @@ def _load_oracle():
     lib.sao_sys_get_draw.argtypes = [_vp]
     lib.sao_sys_set_draw.argtypes = [_vp, _u64]
     lib.sao_sys_set_first_colour.argtypes = [_vp, ctypes.c_int]
+    lib.sao_sys_set_split.argtypes = [_vp, ctypes.c_int]
     for f in ("sao_sys_init_J", "sao_sys_init_rand", "sao_sys_init_order"):
         getattr(lib, f).argtypes = [_vp]
     lib.sao_sys_sweep.argtypes = [_vp, ctypes.c_long]
@@ -221,6 +222,9 @@ class OracleSystem:
 
     def set_first_colour(self, c: int):
         self.lib.sao_sys_set_first_colour(self.h, c)
+
+    def set_split(self, on: bool):
+        self.lib.sao_sys_set_split(self.h, int(bool(on)))
 
     def sweep(self, n: int = 1):
         self.lib.sao_sys_sweep(self.h, n)

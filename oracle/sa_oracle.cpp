@@ -144,6 +144,7 @@ struct OSys {
   // PHILOX state: key, next draw index shared by all sites, spin-init epoch
   uint64_t seed, draw, epoch;
   int first = 0;  // colour of the first half-sweep of a sweep
+  int split = 0;  // the reference's SPLIT_H update (PHILOX mode)
   // MT state
   std::mt19937_64 gen;
   std::uniform_real_distribution<double> uni;
@@ -231,6 +232,51 @@ static void update_site(OSys& o, long i, const Draw& r) {
   o.s[i] = si ^ flip;
 }
 
+// The SPLIT_H update restated from the reference's GPU kernels
+// (src/device_2d.cu:27-50 with the boundary handling of :114-125,
+// src/device_3d.cu:216-245 with :76-89) and tables (src/gpu_2d.cu:133-139,
+// src/gpu_3d.cu:57-63): "exactly k satisfied" masks eq[k]; the bond part of
+// eq[z] / eq[z-1] (and eq[z-2] in 3D) is accepted iff rand1 < the float entry
+// exp(-2 j / T), j = 2k - z (open-x border sites, whose forced bond is in k:
+// j = 2k - 5), every smaller k always; an up spin's field part iff
+// rand2 < float(exp(-2 h / T)). 3D sites on the boundary use rand2 for both.
+static void update_site_split(OSys& o, long i, float r1, float r2) {
+  word_t si = o.s[i];
+  word_t m[6];
+  int nb = 0;
+  bool border = false;
+  if (o.lattice == LAT_3D_PERIODIC) {
+    m[0] = o.Jx[2 * i] ^ si ^ o.s[nb_w(o, i)];
+    m[1] = o.Jx[2 * i + 1] ^ si ^ o.s[nb_e(o, i)];
+    m[2] = o.Jy[2 * i] ^ si ^ o.s[nb_n(o, i)];
+    m[3] = o.Jy[2 * i + 1] ^ si ^ o.s[nb_s(o, i)];
+    m[4] = o.Jz[2 * i] ^ si ^ o.s[nb_u(o, i)];
+    m[5] = o.Jz[2 * i + 1] ^ si ^ o.s[nb_d(o, i)];
+    nb = 6;
+    const long x = i % o.L, y = (i / o.L) % o.L, z = i / o.L2;
+    if (x == 0 || y == 0 || z == 0 || x == o.L - 1 || y == o.L - 1 || z == o.L - 1) r1 = r2;
+  } else {
+    bool xb_lo = (i % o.L == 0), xb_hi = ((i + 1) % o.L == 0);
+    bool open = (o.lattice == LAT_2D_OPEN_X);
+    m[0] = (open && xb_lo) ? ~(word_t)0 : (o.Jx[2 * i] ^ o.s[nb_w(o, i)] ^ si);
+    m[1] = (open && xb_hi) ? ~(word_t)0 : (o.Jx[2 * i + 1] ^ o.s[nb_e(o, i)] ^ si);
+    m[2] = o.Jy[2 * i] ^ o.s[nb_n(o, i)] ^ si;
+    m[3] = o.Jy[2 * i + 1] ^ o.s[nb_s(o, i)] ^ si;
+    nb = 4;
+    border = open && (xb_lo || xb_hi);
+  }
+  word_t eq[7];
+  count_eq(m, nb, eq);
+  word_t bond_ok = 0;
+  for (int k = 0; k <= nb; ++k) {
+    const int j = border ? 2 * k - 5 : 2 * k - nb;
+    const bool acc = (j <= 0) || (r1 < (float)std::exp(-2. * j * (1. / o.T)));
+    if (acc) bond_ok |= eq[k];
+  }
+  const word_t dh = (r2 < (float)std::exp(-2. * o.h / o.T)) ? ~(word_t)0 : 0;
+  o.s[i] = si ^ (bond_ok & (~si | dh));
+}
+
 static void sweep_once(OSys& o) {
   for (int pass = 0; pass < 2; ++pass) {
     const int offset = pass ^ o.first;  // the colour of this half-sweep
@@ -239,6 +285,12 @@ static void sweep_once(OSys& o) {
       for (int y = 0; y < o.L; ++y)
         for (int x = (y + offset) % 2; x < o.L; x += 2) {
           long i = (long)z * o.L2 + (long)y * o.L + x;
+          if (o.split) {
+            const float r1 = uniform_from_u32(philox_draw(o.seed, (uint64_t)i, o.draw + 2 * pass));
+            const float r2 = uniform_from_u32(philox_draw(o.seed, (uint64_t)i, o.draw + 2 * pass + 1));
+            update_site_split(o, i, r1, r2);
+            continue;
+          }
           Draw r;
           if (o.mode == MODE_PHILOX) {
             r.use_float = true;
@@ -252,7 +304,7 @@ static void sweep_once(OSys& o) {
           update_site(o, i, r);
         }
   }
-  if (o.mode == MODE_PHILOX) o.draw += 2;
+  if (o.mode == MODE_PHILOX) o.draw += o.split ? 4 : 2;
 }
 
 // Own bond words (compact, d per site) -> reference layout.
@@ -354,6 +406,8 @@ void sao_sys_set_draw(void* p, uint64_t d) { ((OSys*)p)->draw = d; }
 // colour of each sweep's first half-sweep (PHILOX mode): 1 is the second
 // configuration of the reference GPU systems' two-lattice pair
 void sao_sys_set_first_colour(void* p, int c) { ((OSys*)p)->first = c ? 1 : 0; }
+// the reference's SPLIT_H update (PHILOX mode)
+void sao_sys_set_split(void* p, int on) { ((OSys*)p)->split = on ? 1 : 0; }
 
 void sao_sys_init_J(void* p) {
   OSys* o = (OSys*)p;

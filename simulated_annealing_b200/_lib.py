@@ -60,6 +60,8 @@ _PROTOS = {
     "sa_sys_get_T": (_c.c_int, [_vp, _f64p]),
     "sa_sys_set_first_colour": (_c.c_int, [_vp, _c.c_int]),
     "sa_sys_get_first_colour": (_c.c_int, [_vp, _c.POINTER(_c.c_int)]),
+    "sa_sys_set_split_field": (_c.c_int, [_vp, _c.c_int]),
+    "sa_sys_get_split_field": (_c.c_int, [_vp, _c.POINTER(_c.c_int)]),
     "sa_sys_set_seed": (_c.c_int, [_vp, _u64]),
     "sa_sys_init_J": (_c.c_int, [_vp]),
     "sa_sys_init_rand": (_c.c_int, [_vp]),

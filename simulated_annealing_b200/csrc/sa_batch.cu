@@ -2461,7 +2461,7 @@ int sa_serve_active(sa_serve_t s, int* n, long long* free_words) {
 namespace sa {
 
 bool resident_ok(const sa_system* sy) {
-  return sy->rng_mode == SA_RNG_PHILOX && sy->first_colour == 0 && sy->h == 0.0 && sy->L >= 4 &&
+  return sy->rng_mode == SA_RNG_PHILOX && sy->first_colour == 0 && !sy->split && sy->h == 0.0 && sy->L >= 4 &&
          sy->N <= kBatchMaxN;
 }
 

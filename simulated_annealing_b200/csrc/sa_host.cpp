@@ -64,6 +64,31 @@ uint32_t threshold_of(float b) {
   return lo >= (1ULL << 32) ? 0xFFFFFFFFu : (uint32_t)lo;
 }
 
+uint64_t threshold64_of(float b) {
+  uint64_t lo = 0, hi = 1ULL << 32;
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (uniform_from_u32((uint32_t)mid) < b) lo = mid + 1; else hi = mid;
+  }
+  return lo;  // 2^32 when every u passes (b > 1)
+}
+
+bool make_split_thresholds(int lattice, double T, double h, SplitThresholds* t) {
+  if (!(T > 0)) return false;
+  memset(t, 0, sizeof *t);
+  const int z = (lattice == SA_LATTICE_3D) ? 6 : 4;
+  // the reference's table entries: float(exp(-2.*j*(1./T))) for j = 2n - z
+  auto entry = [&](int j) -> uint64_t {
+    if (j <= 0) return 1ULL << 32;  // the reference accepts these without a draw
+    return threshold64_of((float)std::exp(-2. * j * (1. / T)));
+  };
+  for (int n = 0; n <= z; ++n) t->bond[n] = entry(2 * n - z);
+  if (lattice != SA_LATTICE_3D)
+    for (int n = 0; n <= 4; ++n) t->bbond[n] = entry(2 * n - 5);  // the forced bond counts in n
+  t->field = threshold64_of((float)std::exp(-2. * h / T));
+  return true;
+}
+
 bool make_thresholds(int lattice, double T, double h, Thresholds* t) {
   double b[20];
   boltz_table(lattice, T, h, b);

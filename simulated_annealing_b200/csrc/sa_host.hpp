@@ -34,6 +34,13 @@ uint32_t threshold_of(float b);
 // Integer thresholds of a lattice at (T, h): float-cast table, then thr().
 // Returns false if the table is not monotone where the kernels need it.
 bool make_thresholds(int lattice, double T, double h, Thresholds* out);
+// #{u : uniform(u) < b} for any float b (2^32 when b > 1)
+uint64_t threshold64_of(float b);
+// The split tables (src/gpu_2d.cu:133-139, src/gpu_3d.cu:57-63): the bond
+// part for n satisfied of z bonds costs 2(2n - z) (border sites 2(2n - 5)),
+// accepted always when that is <= 0, else with float(exp(-2 j / T)); the
+// field part float(exp(-2 h / T)), not clamped to 1.
+bool make_split_thresholds(int lattice, double T, double h, SplitThresholds* out);
 // Tables for the mt19937_64 stream (see ThresholdsMT).
 bool make_thresholds_mt(int lattice, double T, double h, ThresholdsMT* out);
 // The reference CPU classes' uniform: u(g) for a 64-bit generator output.

@@ -168,7 +168,7 @@ extern "C" int sa_sys_anneal(sa_system_t sy, const double* T, int nsteps, int sw
     if (!(T[k] > 0)) return fail(SA_ERR_INVALID, "temperatures must be > 0");
     if (!make_thresholds(sy->lattice, T[k], sy->h, &thr[k])) return fail(SA_ERR_INVALID, "non-monotone table");
   }
-  if (sy->rng_mode == SA_RNG_MT19937_64 || sy->first_colour != 0) {
+  if (sy->rng_mode == SA_RNG_MT19937_64 || sy->first_colour != 0 || sy->split) {
     // the CPU reference's stream, or a system whose sweeps start with colour
     // 1: annealing<>'s own loop (src/annealing.hpp:67-100) over sa_sys_sweep /
     // sa_sys_measure

@@ -39,15 +39,32 @@ __device__ __forceinline__ uint32_t prefix_count_mt(uint64_t g, const uint64_t* 
   return t;
 }
 
+// The split update (the reference's SPLIT_H build, src/device_2d.cu:27-50,
+// src/device_3d.cu:216-245): with n satisfied bonds (bit-sliced c2 c1 c0),
+// the bond part is accepted iff u1 < bond[n] -- the accepted n are a prefix
+// of 0..NB because bond[] does not increase -- and an up spin's field part
+// iff u2 < field; a replica flips when both parts are accepted.
+template <int NB>
+__device__ __forceinline__ word_t split_flip(word_t si, word_t c0, word_t c1, word_t c2, uint32_t u1, uint32_t u2,
+                                             const uint64_t* bond, uint64_t field) {
+  uint32_t tb = 0;
+#pragma unroll
+  for (int n = 0; n <= NB; ++n) tb += ((uint64_t)u1 < bond[n]) ? 1u : 0u;
+  const word_t bond_ok = ~ge_scalar(c0, c1, c2, tb);           // n < tb
+  const word_t field_ok = ~si | bcast((uint64_t)u2 < field);  // down spins: always
+  return si ^ (bond_ok & field_ok);
+}
+
 // MT: the site's draw is the pass's mt19937_64 output at its rank in the
 // reference's sweep order (draws[idx], idx = row * L/2 + k), not Philox.
-template <bool OPEN_X, bool MT = false>
+// SPLIT: the split update with draws `draw` (bond) and `draw + 1` (field).
+template <bool OPEN_X, bool MT = false, bool SPLIT = false>
 __global__ void __launch_bounds__(256) k_halfsweep_2d(word_t* __restrict__ s,
                                                       const word_t* __restrict__ J, int L,
                                                       unsigned long long seed,
                                                       unsigned long long draw, int c,
                                                       Thresholds thr, const uint64_t* __restrict__ draws = nullptr,
-                                                      ThresholdsMT tm = {}) {
+                                                      ThresholdsMT tm = {}, SplitThresholds st = {}) {
   const int hL = L >> 1;
   const long half = (long)L * hL;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -77,6 +94,12 @@ __global__ void __launch_bounds__(256) k_halfsweep_2d(word_t* __restrict__ s,
   }
   word_t c0, c1, c2;
   count4(mw, me, mn, ms, c0, c1, c2);
+  if (SPLIT) {
+    const unsigned long long site = (unsigned long long)x + (unsigned long long)L * y;
+    const uint32_t u1 = philox_draw(seed, site, draw), u2 = philox_draw(seed, site, draw + 1);
+    sc[idx] = split_flip<4>(si, c0, c1, c2, u1, u2, (OPEN_X && border) ? st.bbond : st.bond, st.field);
+    return;
+  }
   uint32_t tdn, tup;
   if (MT) {
     const uint64_t g = draws[idx];
@@ -102,13 +125,16 @@ __global__ void __launch_bounds__(256) k_halfsweep_2d(word_t* __restrict__ s,
 }
 
 // One 3D half-sweep of colour c; one thread per (x,y) column, walking z.
-template <bool MT = false>
+// SPLIT: the split update; a site on the lattice's boundary (a coordinate 0
+// or L-1) uses its field draw for the bond part too, as the reference's
+// boundary branch passes rand2 twice (src/device_3d.cu:76-89).
+template <bool MT = false, bool SPLIT = false>
 __global__ void __launch_bounds__(128) k_halfsweep_3d(word_t* __restrict__ s,
                                                       const word_t* __restrict__ J, int L,
                                                       unsigned long long seed,
                                                       unsigned long long draw, int c,
                                                       Thresholds thr, const uint64_t* __restrict__ draws = nullptr,
-                                                      ThresholdsMT tm = {}) {
+                                                      ThresholdsMT tm = {}, SplitThresholds st = {}) {
   const int hL = L >> 1;
   const long plane = (long)L * hL;  // columns per colour
   const long half = plane * L;
@@ -143,6 +169,17 @@ __global__ void __launch_bounds__(128) k_halfsweep_3d(word_t* __restrict__ s,
     word_t md = Jz_c[rd * hL + k] ^ sd ^ si;
     word_t c0, c1, c2;
     count6(mw, me, mn, ms, mu, md, c0, c1, c2);
+    if (SPLIT) {
+      const unsigned long long site = (unsigned long long)x + (unsigned long long)L * r;
+      const uint32_t u2 = philox_draw(seed, site, draw + 1);
+      const bool edge = x == 0 || y == 0 || z == 0 || x == L - 1 || y == L - 1 || z == L - 1;
+      const uint32_t u1 = edge ? u2 : philox_draw(seed, site, draw);
+      const word_t ns = split_flip<6>(si, c0, c1, c2, u1, u2, st.bond, st.field);
+      sc[idx] = ns;
+      if (z == 0) first = ns;
+      prev = ns;
+      continue;
+    }
     uint32_t tdn, tup;
     if (MT) {
       const uint64_t g = draws[idx];
@@ -329,6 +366,20 @@ __global__ void k_split_to_rowmajor(const word_t* __restrict__ src, word_t* __re
 static inline unsigned grid_for(long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 int launch_halfsweep(sa_system* sy, int c, unsigned long long draw) {
+  if (sy->split) {
+    if (sy->lattice == SA_LATTICE_3D) {
+      long plane = (long)sy->L * (sy->L / 2);
+      k_halfsweep_3d<false, true><<<grid_for(plane, 128), 128, 0, sy->stream>>>(
+          sy->d_s, sy->d_J, sy->L, sy->seed, draw, c, sy->thr, nullptr, ThresholdsMT{}, sy->sthr);
+    } else if (sy->lattice == SA_LATTICE_2D_OPEN_X) {
+      k_halfsweep_2d<true, false, true><<<grid_for(sy->half, 256), 256, 0, sy->stream>>>(
+          sy->d_s, sy->d_J, sy->L, sy->seed, draw, c, sy->thr, nullptr, ThresholdsMT{}, sy->sthr);
+    } else {
+      k_halfsweep_2d<false, false, true><<<grid_for(sy->half, 256), 256, 0, sy->stream>>>(
+          sy->d_s, sy->d_J, sy->L, sy->seed, draw, c, sy->thr, nullptr, ThresholdsMT{}, sy->sthr);
+    }
+    return SA_OK;
+  }
   if (sy->lattice == SA_LATTICE_3D) {
     long plane = (long)sy->L * (sy->L / 2);
     k_halfsweep_3d<false><<<grid_for(plane, 128), 128, 0, sy->stream>>>(sy->d_s, sy->d_J, sy->L, sy->seed,
@@ -507,6 +558,7 @@ int sa_sys_set_T(sa_system_t sy, double T) {
   sy->T = T;
   sy->thr = t;  // kernel argument: later launches see it, earlier ones keep theirs
   if (sy->rng_mode == SA_RNG_MT19937_64) sy->thr_mt = tm;
+  make_split_thresholds(sy->lattice, sy->T, sy->h, &sy->sthr);
   return SA_OK;
 }
 
@@ -520,6 +572,7 @@ int sa_sys_set_h(sa_system_t sy, double h) {
   sy->h = h;
   sy->thr = t;
   if (sy->rng_mode == SA_RNG_MT19937_64) sy->thr_mt = tm;
+  make_split_thresholds(sy->lattice, sy->T, sy->h, &sy->sthr);
   return SA_OK;
 }
 
@@ -551,6 +604,8 @@ int sa_sys_set_seed(sa_system_t sy, uint64_t seed) {
 int sa_sys_set_rng_mode(sa_system_t sy, int mode) {
   if (!sy) return fail(SA_ERR_INVALID, "null system");
   if (mode != SA_RNG_PHILOX && mode != SA_RNG_MT19937_64) return fail(SA_ERR_INVALID, "unknown random mode");
+  if (mode == SA_RNG_MT19937_64 && sy->split)
+    return fail(SA_ERR_UNSUPPORTED, "the split update is defined for the GPU reference's Philox draws only");
   if (mode == SA_RNG_MT19937_64 && sy->first_colour != 0)
     return fail(SA_ERR_UNSUPPORTED, "the mt19937_64 stream has one visiting order: first colour must be 0");
   if (mode == SA_RNG_MT19937_64) {
@@ -571,6 +626,21 @@ int sa_sys_set_first_colour(sa_system_t sy, int colour) {
   if (colour != 0 && sy->rng_mode != SA_RNG_PHILOX)
     return fail(SA_ERR_UNSUPPORTED, "the first colour can be 1 in Philox mode only");
   sy->first_colour = colour;
+  return SA_OK;
+}
+
+int sa_sys_set_split_field(sa_system_t sy, int on) {
+  if (!sy) return fail(SA_ERR_INVALID, "null system");
+  if (on && sy->rng_mode != SA_RNG_PHILOX)
+    return fail(SA_ERR_UNSUPPORTED, "the split update is defined for the GPU reference's Philox draws only");
+  sy->split = on ? 1 : 0;
+  make_split_thresholds(sy->lattice, sy->T, sy->h, &sy->sthr);
+  return SA_OK;
+}
+
+int sa_sys_get_split_field(sa_system_t sy, int* on) {
+  if (!sy || !on) return fail(SA_ERR_INVALID, "null argument");
+  *on = sy->split;
   return SA_OK;
 }
 
@@ -722,10 +792,11 @@ int sa_sys_sweep(sa_system_t sy, long nsweeps) {
     return resident_run(sy, &T, 1, (int)nsweeps, 0, nullptr, nullptr, nullptr);
   }
   const int c0 = sy->first_colour;
+  const int per = sy->split ? 2 : 1;  // draws per site per half-sweep
   for (long k = 0; k < nsweeps; ++k) {
     launch_halfsweep(sy, c0, sy->draw);
-    launch_halfsweep(sy, 1 - c0, sy->draw + 1);
-    sy->draw += 2;
+    launch_halfsweep(sy, 1 - c0, sy->draw + per);
+    sy->draw += 2 * per;
   }
   SA_CUDA_TRY(cudaGetLastError());
   return SA_OK;
@@ -812,7 +883,7 @@ int sa_sys_device_buffers(sa_system_t sy, uint64_t** d_spins, uint64_t** d_J) {
 // internal spins (N words) and own couplings (dim*N words).
 struct CkptHeader {
   char magic[8];
-  int32_t version, lattice, L, pad;  // pad: the first colour
+  int32_t version, lattice, L, pad;  // pad: bit 0 the first colour, bit 1 the split update
   double T, h;
   uint64_t seed, draw, epoch;
 };
@@ -828,7 +899,7 @@ int sa_sys_save(sa_system_t sy, void* buf, size_t cap, size_t* len) {
   memset(&hd, 0, sizeof hd);
   memcpy(hd.magic, "SAB200CK", 8);
   hd.version = mt_bytes ? 2 : 1;  // 2: mt19937_64 mode, generator state appended
-  hd.pad = sy->first_colour;      // 0 in records written before the field existed
+  hd.pad = sy->first_colour | (sy->split << 1);  // 0 in records written before these existed
   hd.lattice = sy->lattice;
   hd.L = sy->L;
   hd.T = sy->T;
@@ -885,7 +956,9 @@ int sa_sys_load(sa_system_t sy, const void* buf, size_t len) {
   sy->seed = hd.seed;
   sy->draw = hd.draw;
   sy->epoch = hd.epoch;
-  sy->first_colour = (hd.pad == 1 && !mt) ? 1 : 0;
+  sy->first_colour = ((hd.pad & 1) && !mt) ? 1 : 0;
+  sy->split = ((hd.pad & 2) && !mt) ? 1 : 0;
+  make_split_thresholds(sy->lattice, sy->T, sy->h, &sy->sthr);
   return SA_OK;
 }
 

@@ -26,6 +26,10 @@ struct sa_system {
   // systems' two-lattice pair (src/gpu_2d.cu:109-120): its odd sites are
   // updated first. Philox mode only.
   int first_colour = 0;
+  // The reference's SPLIT_H update (bond and field parts accepted with two
+  // draws per site per half-sweep: t+2m and t+2m+1); Philox mode only.
+  int split = 0;
+  sa::SplitThresholds sthr{};
   uint64_t* d_mt = nullptr;        // [kMtN + 1]: state words, next index
   uint64_t* d_draws = nullptr;     // dim * N outputs (init_J is the largest pass)
   sa::ThresholdsMT thr_mt{};

@@ -32,6 +32,20 @@ struct ThresholdsMT {
   int ndn, nup, nbdn, nbup;
 };
 
+// The split acceptance (the reference's SPLIT_H build, src/device_2d.cu:27-50,
+// src/device_3d.cu:216-245): the bond part of a flip is accepted with one
+// uniform, the field part of an up spin with a second. bond[n] / bbond[n]
+// (open-x border sites, whose forced bond is counted in n): the bond part of
+// a replica with n satisfied bonds is accepted iff u1 < bond[n] (2^32:
+// always); field: an up spin's field part iff u2 < field. Thresholds are
+// counts of u32 values whose uniform lies below the float table entry, as
+// in Thresholds, but 64-bit so that "always" (an entry above 1) fits.
+struct SplitThresholds {
+  uint64_t bond[8];
+  uint64_t bbond[8];
+  uint64_t field;
+};
+
 // mt19937_64 (Matsumoto & Nishimura, the C++ standard's predefined engine):
 // 312 state words; the state block on the device holds the words and then
 // the index of the next output.

@@ -110,6 +110,16 @@ class GpuSystem:
         two-lattice pair. Philox mode only."""
         check(self._lib.sa_sys_set_first_colour(self._h, int(colour)))
 
+    def set_split_field(self, on: bool) -> None:
+        """The reference's SPLIT_H update: bond and field parts of a flip
+        accepted with two draws (sa_sys_set_split_field). Philox mode only."""
+        check(self._lib.sa_sys_set_split_field(self._h, int(bool(on))))
+
+    def split_field(self) -> bool:
+        c = ctypes.c_int()
+        check(self._lib.sa_sys_get_split_field(self._h, ctypes.byref(c)))
+        return bool(c.value)
+
     def first_colour(self) -> int:
         c = ctypes.c_int()
         check(self._lib.sa_sys_get_first_colour(self._h, ctypes.byref(c)))
