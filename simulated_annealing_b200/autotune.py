@@ -5,7 +5,7 @@ batch of that shape with every candidate shape -- cluster size C (the
 smallest whose shared memory fits, and the next three larger ones), slots
 per lane SL (1, or 2 for an even slot count), the two-slot 3D walk's
 high-register form, warps per block (3 up to one pass over the CTA's
-columns) -- against the engine's built-in heuristics, and keeps a shape only
+columns, two at least) -- against the engine's built-in heuristics, and keeps a shape only
 where it beats them. Results go to a JSON record and to the table compiled
 into the library (csrc/sa_tuning.inc):
 
@@ -68,8 +68,9 @@ def candidates(lat, L, nslots):
                 # tiles of 32 sites (the rp lanes of a site inside a tile)
                 passes = max(1, -(-(cols * rp) // 32)) if lat == LAT_3D else max(1, -(-cols // 32))
                 # several small blocks per SM often beat one large one: from
-                # 3 warps up to one pass over the CTA's work (or the cap)
-                top = min(cap, passes)
+                # 3 warps up to one pass over the CTA's work (or the cap); two
+                # warps at least (threads 0..63 hold one replica each)
+                top = max(2, min(cap, passes))
                 ws = sorted({w for w in (3, 4, 5, 6, 7, 8, 10, 12, 16, 20) if w <= top} | {top})
                 for w in ws:
                     out.append((lat, L, nslots, C, SL, w, hr))
@@ -120,12 +121,16 @@ def main():
     ap.add_argument("--margin", type=float, default=0.01, help="keep a shape only if this much faster")
     ap.add_argument("--buckets", choices=["mix", "serve", "all"], default="all")
     ap.add_argument("--keep", default=None, help="a JSON record whose table entries for other buckets are kept")
+    ap.add_argument("--only", nargs="+", default=None, metavar="LAT:L:SLOTS",
+                    help="tune these buckets instead of a --buckets set (e.g. 2:8:1)")
     args = ap.parse_args()
     stream = torch.cuda.Stream()
     record = {"device": torch.cuda.get_device_name(0), "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
               "instances": args.instances, "sweeps": args.sweeps, "buckets": []}
     table = []
     buckets = {"mix": BUCKETS, "serve": SERVE_BUCKETS, "all": BUCKETS + SERVE_BUCKETS}[args.buckets]
+    if args.only:
+        buckets = [tuple(int(v) for v in b.split(":")) for b in args.only]
     if args.keep:
         old = json.load(open(args.keep))
         mine = {tuple(b) for b in buckets}

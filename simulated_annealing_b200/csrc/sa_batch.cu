@@ -579,8 +579,9 @@ __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG, HR>(), 1) k_r
         const int nh = (a + 1 < d.nslots) ? 2 : 1;
         rmeasure<CL>(x, d3, open, a, nh, s_cnt);
         sync_all();
-        if (q == 0 && threadIdx.x < 64 * nh) {
-          const int qq = threadIdx.x >> 6, j = threadIdx.x & 63;
+        // a 64-thread CTA folds two slots in two rounds
+        for (int t = threadIdx.x; q == 0 && t < 64 * nh; t += blockDim.x) {
+          const int qq = t >> 6, j = t & 63;
           unsigned v = 0;
           if (CL) {
             for (int r = 0; r < C; ++r) v += cluster.map_shared_rank(&s_cnt[0][0], (unsigned)r)[qq * 64 + j];
@@ -1005,14 +1006,17 @@ static const std::vector<TuneEntry>& builtin_tuning() {
 }
 
 // A tuned shape usable for instance d at cluster size C (the shape's C fits
-// the shared-memory budget, SL = 2 only for an even slot count); else null.
+// the shared-memory budget, SL = 2 only for an even slot count, two warps at
+// least); else null.
 static const TuneEntry* tune_for(const sa_batch* b, const InstDesc& d) {
   const std::vector<TuneEntry>& t = b->tuning_set ? b->tuning : builtin_tuning();
   for (const TuneEntry& e : t) {
     if (e.lattice != d.lattice || e.L != d.L || e.nslots != d.nslots) continue;
     if (e.C < 1 || e.C > std::min(16, d.L) || resident_bytes(d, e.C) > kResSmemBudget) return nullptr;
     if (e.SL != 1 && (e.SL != 2 || d.nslots % 2 != 0)) return nullptr;
-    if (e.warps < 1) return nullptr;
+    // threads 0..63 of a resident CTA hold one replica each (anneal record,
+    // exchange decision): two warps at least
+    if (e.warps < 2) return nullptr;
     return &e;
   }
   return nullptr;
@@ -1093,7 +1097,7 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
         const int wmax = g.hr ? kHiRegThreads / 32
                               : (d.lattice == SA_LATTICE_3D && g.SL == 1 && g.RP == 1) ? kSegMaxThreads / 32
                                                                                        : kResMaxWarps;
-        g.threads = 32 * std::max(1, std::min(te->warps, wmax));
+        g.threads = 32 * std::max(2, std::min(te->warps, wmax));
       } else if (C && !wide) {
         // warp passes of one half-sweep: 3D walks columns, 32/RP per pass; 2D
         // takes tiles of 32 sites (RP sub-steps of 32/RP sites each). Two slots

@@ -36,6 +36,7 @@ def test_table_and_record_agree():
     rows = _inc_rows()
     for r in rows:
         assert len(r) == 7 and r[0] in (0, 1, 2) and r[1] % 2 == 0 and r[3] >= 1 and r[4] in (1, 2)
+        assert r[5] >= 2  # threads 0..63 hold one replica each
     if os.path.exists(JSON):
         rec = json.load(open(JSON))
         assert [list(map(int, e)) for e in rec["table"]] == rows
