@@ -61,9 +61,15 @@ def candidates(lat, L, nslots):
                 rp <<= 1
             his = [0, 1] if (SL == 2 and lat == LAT_3D) else [0]
             for hr in his:
-                # the engine's caps: 12 warps for the high-register form, 16 for
-                # single-slot 3D (its walk keeps more words live), else 20
-                cap = 12 if hr else (16 if (lat == LAT_3D and SL == 1 and rp == 1) else 20)
+                # the engine's caps: 12 warps for the high-register form, 8 for
+                # two-slot 2D lanes in clusters, 16 for single-slot 3D (its walk
+                # keeps more words live), else 20
+                if hr:
+                    cap = 12
+                elif lat != LAT_3D and SL == 2 and C > 1:
+                    cap = 8
+                else:
+                    cap = 16 if (lat == LAT_3D and SL == 1 and rp == 1) else 20
                 # 3D: one lane group of rp lanes per column; 2D: warps take
                 # tiles of 32 sites (the rp lanes of a site inside a tile)
                 passes = max(1, -(-(cols * rp) // 32)) if lat == LAT_3D else max(1, -(-cols // 32))

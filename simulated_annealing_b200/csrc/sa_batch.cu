@@ -365,11 +365,27 @@ __global__ void __launch_bounds__(kBatchThreads, 1) k_batch(BatchParams p) {
 // than one CTA (DSMEM halos and cluster barriers) or single CTAs (block
 // barriers only).
 // Single-slot 3D variants (segmented walk, fused measurement) hold more state
-// per thread: 16 warps at up to 128 registers.
-template <int P, int SL, int LAT, bool SEG, bool HR = false>
+// per thread: 16 warps at up to 128 registers. Clustered two-slot 2D blocks:
+// 8 warps, two blocks per SM.
+template <int P, int SL, int LAT, bool CL, bool SEG, bool HR = false>
 constexpr int res_max_threads() {
-  return HR ? kHiRegThreads
-            : (SEG || (P == 1 && SL == 1 && LAT == SA_LATTICE_3D)) ? kSegMaxThreads : kResMaxThreads;
+  return HR                                          ? kHiRegThreads
+         : (LAT != SA_LATTICE_3D && SL == 2 && CL)   ? kRes2dClThreads
+         : (SEG || (P == 1 && SL == 1 && LAT == SA_LATTICE_3D)) ? kSegMaxThreads
+                                                                : kResMaxThreads;
+}
+template <int SL, int LAT, bool CL, bool HR>
+constexpr int res_min_blocks() {
+  return (!HR && LAT != SA_LATTICE_3D && SL == 2 && CL) ? 2 : 1;
+}
+
+// The host's cap on warps per block for a resident group, matching the
+// kernel's launch bounds above.
+static int res_warp_cap(int lattice, int SL, int RP, int C, bool hr, bool seg) {
+  if (hr) return kHiRegThreads / 32;
+  if (lattice != SA_LATTICE_3D && SL == 2 && C > 1) return kRes2dClThreads / 32;
+  if (seg || (lattice == SA_LATTICE_3D && SL == 1 && RP == 1)) return kSegMaxThreads / 32;
+  return kResMaxWarps;
 }
 
 // SEG: single-slot 3D instances spread over many SMs walk their columns in
@@ -379,7 +395,8 @@ constexpr int res_max_threads() {
 // keeps twice the words live; where a CTA has work for few warps anyway this
 // trades nothing for no spills).
 template <int P, int SL, int LAT, bool CL, bool SEG = false, bool HR = false>
-__global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG, HR>(), 1) k_resident(BatchParams p) {
+__global__ void __launch_bounds__(res_max_threads<P, SL, LAT, CL, SEG, HR>(), res_min_blocks<SL, LAT, CL, HR>())
+    k_resident(BatchParams p) {
   extern __shared__ __align__(16) word_t s_spins[];
   __shared__ unsigned s_cnt[2][64];   // this CTA's partial counts
   __shared__ unsigned s_mask[2];
@@ -526,6 +543,9 @@ __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG, HR>(), 1) k_r
     const bool xchg = d.ladder >= 0 && d.nslots > 1 && (sweeps + 1) % p.xinterval == 0;
     Decision dc = {0, 0, 0, 0};
     if (xchg) dc = p.dec[d.dec_off + xsteps];
+    // 2D: each warp counts the pair's energies after its colour-1 walk
+    // (rmeasure_own_2d), unless a histogram pass needs s_cnt first
+    const bool own = !d3 && xchg && !(p.hist && d.hist_off >= 0 && (sweeps + 1) % p.hstride == 0);
     if (d.sched >= 0) {
       int64_t s = sweeps / d.sweeps_per_step;
       if (s > d.thr_count - 1) s = d.thr_count - 1;
@@ -549,10 +569,13 @@ __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG, HR>(), 1) k_r
           const int cmode = !fuse ? 0 : (c == 0 ? (pending ? 1 : 0) : (meas_now ? 2 : 0));
           rhalf_3d1<2, CL>(x, c, draw + c, th[0], &bc, cmode);
         } else {
-          rhalf_3d<P, SL, CL>(x, c, draw + c, th);
+          rhalf_3d<P, SL, CL, HR>(x, c, draw + c, th);
         }
       }
-      else rhalf_2d<P, SL, open, CL>(x, c, draw + c, th, tb);
+      else {
+        rhalf_2d<P, SL, open, CL>(x, c, draw + c, th, tb);
+        if (own && c == 1) rmeasure_own_2d<open, CL>(x, dc.pair, s_cnt);
+      }
       sync_all();
       if (fuse && c == 0 && pending) {
         // the previous sweep's count is complete: reduce it over the CTA
@@ -607,9 +630,13 @@ __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, SEG, HR>(), 1) k_r
         nsl = 2;
       }
       // s_cnt was zeroed at the start of this sweep unless a histogram pass
-      // used it since; four units' loads in flight per lane
-      rmeasure<CL, 4>(x, d3, open, a, nsl, s_cnt, hist_now);
-      sync_all();
+      // used it since; four units' loads in flight per lane. The 2D pair
+      // counts are already there (own): the barrier after the colour-1 half
+      // made them complete.
+      if (!own) {
+        rmeasure<CL, 4>(x, d3, open, a, nsl, s_cnt, hist_now);
+        sync_all();
+      }
       if (xchg) {
         // every CTA of the cluster reaches the same decision from the
         // cluster's totals: 64 threads, one replica each, then one barrier
@@ -1094,9 +1121,7 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
         g.RP = 1;
         while (g.RP * g.SL < d.nslots) g.RP <<= 1;
         g.hr = te->SL == 2 && te->hr && d.lattice == SA_LATTICE_3D;
-        const int wmax = g.hr ? kHiRegThreads / 32
-                              : (d.lattice == SA_LATTICE_3D && g.SL == 1 && g.RP == 1) ? kSegMaxThreads / 32
-                                                                                       : kResMaxWarps;
+        const int wmax = res_warp_cap(d.lattice, g.SL, g.RP, C, g.hr, false);
         g.threads = 32 * std::max(2, std::min(te->warps, wmax));
       } else if (C && !wide) {
         // warp passes of one half-sweep: 3D walks columns, 32/RP per pass; 2D
@@ -1122,8 +1147,7 @@ static std::vector<int32_t> build_groups(sa_batch* b) {
           }
         }
         const int passes = passes_for(g.RP);
-        const bool big_regs = seg || (d.lattice == SA_LATTICE_3D && g.SL == 1 && g.RP == 1);
-        const int wmax = big_regs ? kSegMaxThreads / 32 : kResMaxWarps;
+        const int wmax = res_warp_cap(d.lattice, g.SL, g.RP, C, false, seg);
         int warps = std::min(passes, wmax);
         const int rounds = (passes + warps - 1) / warps;
         warps = std::max(4, (passes + rounds - 1) / rounds);

@@ -33,6 +33,10 @@ constexpr int kResMaxThreads = kResMaxWarps * 32;
 constexpr int kSegMaxThreads = 512;
 // the high-register form of the two-slot 3D walk: 12 warps, ~170 registers
 constexpr int kHiRegThreads = 384;
+// two-slot 2D lanes in clusters of two or more CTAs (the large 2D lattices):
+// at most 8 warps, launched for two blocks per SM, so up to 128 registers and
+// the walk's words stay in registers (at 96 registers they spilled)
+constexpr int kRes2dClThreads = 256;
 
 struct ResCtx {
   word_t* sm;           // this CTA's rows
@@ -294,7 +298,10 @@ __device__ __forceinline__ void rhalf_2d(const ResCtx& x, int c, uint64_t draw, 
   }
 }
 
-template <int P, int SL, bool CL>
+// DB (the high-register form, which has registers to spare): the next plane
+// block's Philox draw and coupling words are fetched while this block walks,
+// so the L2 round trip of every block but the first is hidden.
+template <int P, int SL, bool CL, bool DB = false>
 __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, const uint32_t (*th)[8]) {
   constexpr int SPS = 32 / P;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -340,27 +347,39 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
     SlotWords<SL> cur = {};
     if (valid) cur = ldw<SL>(x.sm + own);
     word_t jnext = __ldg(Jzc + jo);  // the z-1 coupling of the next plane (plane 0: the wrapped bond)
+    // Lane (column cl, i) draws the Philox number and loads the coupling
+    // words of plane z0+i of a block; the column's P lanes share them by
+    // shuffles, so each coupling word is loaded once per site instead of once
+    // per slot. A plane's z-1 coupling is the z+1 coupling of the plane below;
+    // plane 0's (the wrapped bond) every lane loads before the walk.
+    auto fetch = [&](int z0, uint32_t& u_, word_t& w_, word_t& e_, word_t& n_, word_t& s_, word_t& d_) {
+      const int zd = z0 + (lane % P);
+      u_ = 0;
+      w_ = e_ = n_ = s_ = d_ = 0;
+      if (col_ok && zd < L) {
+        const int zo = zd * zg;
+        w_ = __ldg(Jxc + jo + zo);
+        e_ = __ldg(Jxo + je + zo);
+        n_ = __ldg(Jyc + jo + zo);
+        s_ = __ldg(Jyo + js + zo);
+        d_ = __ldg(Jzc + jo + ((zd == L - 1) ? 0 : zo + zg));
+        u_ = philox_draw(x.seed, (unsigned long long)(xx + L * (y + L * zd)), draw);
+      }
+    };
+    uint32_t um = 0;
+    word_t bw = 0, be = 0, bn = 0, bs = 0, bd = 0;
+    if constexpr (DB) fetch(0, um, bw, be, bn, bs, bd);
     // A warp whose lanes all have a site and a slot (every warp of the
     // batched ensembles) walks without the per-lane test.
     auto walk = [&](auto check) {
     constexpr bool CHECK = decltype(check)::value;
     for (int z0 = 0; z0 < L; z0 += P) {
-      // Lane (column cl, i) draws the Philox number and loads the coupling
-      // words of plane z0+i; the column's P lanes share them by shuffles, so
-      // each coupling word is loaded once per site instead of once per slot.
-      // A plane's z-1 coupling is the z+1 coupling of the plane below; plane
-      // 0's (the wrapped bond) every lane loads before the walk.
-      const int zd = z0 + (lane % P);
-      uint32_t um = 0;
-      word_t bw = 0, be = 0, bn = 0, bs = 0, bd = 0;
-      if (col_ok && zd < L) {
-        um = philox_draw(x.seed, (unsigned long long)(xx + L * (y + L * zd)), draw);
-        const int zo = zd * zg;
-        bw = __ldg(Jxc + jo + zo);
-        be = __ldg(Jxo + je + zo);
-        bn = __ldg(Jyc + jo + zo);
-        bs = __ldg(Jyo + js + zo);
-        bd = __ldg(Jzc + jo + ((zd == L - 1) ? 0 : zo + zg));
+      [[maybe_unused]] uint32_t um2 = 0;
+      [[maybe_unused]] word_t bw2 = 0, be2 = 0, bn2 = 0, bs2 = 0, bd2 = 0;
+      if constexpr (DB) {
+        if (z0 + P < L) fetch(z0 + P, um2, bw2, be2, bn2, bs2, bd2);
+      } else {
+        fetch(z0, um, bw, be, bn, bs, bd);
       }
       // One plane. POS 1: plane 0 (its new words are the top plane's z+1
       // neighbours); 2: plane L-1 (its z+1 neighbour is the new plane 0);
@@ -417,6 +436,14 @@ __device__ __forceinline__ void rhalf_3d(const ResCtx& x, int c, uint64_t draw, 
 #pragma unroll 4
       for (; zi < zend; ++zi) step(zi, std::integral_constant<int, 0>{});
       if (top) step(nz - 1, std::integral_constant<int, 2>{});
+      if constexpr (DB) {
+        um = um2;
+        bw = bw2;
+        be = be2;
+        bn = bn2;
+        bs = bs2;
+        bd = bd2;
+      }
     }
     };
     if (__all_sync(0xffffffffu, valid)) walk(std::false_type{});
@@ -931,6 +958,92 @@ __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, in
   }
   if (nsl == 2) rmeasure_body<CL, UNR, 2, 5>(x, d3, open, a, cnt);
   else rmeasure_body<CL, UNR, 1, 5>(x, d3, open, a, cnt);
+}
+
+// ---------------------------------------------------------------------------
+// The exchange pair's satisfied-bond counts in 2D, taken by each warp over its
+// own sites right after its colour-1 walk, with no barrier and no separate
+// pass. Every 2D bond joins a colour-0 and a colour-1 site, so the colour-1
+// sites' four bonds (west and east across an open x edge excepted) cover the
+// lattice once. They are final when this warp has walked its colour-1 tiles:
+// colour 0 was final at the barrier before the colour-1 half, and only this
+// warp writes the colour-1 sites of its tiles (rhalf_2d's tiles: 32 sites
+// from 32 * warp, stepping 32 * warps). Lanes: 16 sites x slots a, a+1; the
+// counts go into cnt[slot - a][replica], as rmeasure's do. (In 3D the same
+// scheme needs the z-bonds of both colours and measured slower than the
+// separate pass.)
+// ---------------------------------------------------------------------------
+template <int W0>
+__device__ __forceinline__ void add3_w(VCount<16>& big, word_t c0, word_t c1, word_t c2) {
+  word_t carry = 0;
+#pragma unroll
+  for (int b = 0; b < W0; ++b) {
+    const word_t q = (b == 0) ? c0 : (b == 1) ? c1 : (b == 2) ? c2 : 0;
+    const word_t a = big.p[b];
+    big.p[b] = a ^ q ^ carry;
+    carry = (a & q) | (carry & (a ^ q));
+  }
+}
+
+template <int W0>
+__device__ __forceinline__ void flush_pair_counts(VCount<16>& big, unsigned (*cnt)[64]) {
+  const int lane = threadIdx.x & 31;
+  warp_sum_grow<2, W0>(big);
+  constexpr int NBU = W0 + 4;
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const int j = (lane >> 1) + 16 * m;
+    atomicAdd(&cnt[lane & 1][j], big.template count_low<NBU>(j));
+  }
+  big.clear();
+}
+
+template <bool OPEN_X, bool CL>
+__device__ __forceinline__ void rmeasure_own_2d(const ResCtx& x, int a, unsigned (*cnt)[64]) {
+  constexpr int W0 = 5;  // a lane adds at most 4 per site: a warp sum every 7 sites
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane >> 1, slot = a + (lane & 1);
+  const int L = x.L, hL = x.hL, ns = x.ns, tot = x.ny * hL;
+  const word_t* J = x.J;
+  VCount<16> big;
+  big.clear();
+  int held = 0;  // sites added since the last warp sum (warp-uniform)
+  for (int base = warp * 32; base < tot; base += nwarps * 32) {
+    for (int h = 0; h < 32; h += 16) {
+      const int t = base + h + g;
+      const bool ok = t < tot;
+      const int tt = ok ? t : base;  // lanes past the end read a real site and count nothing
+      const int yl = div_hl(tt, x);
+      const int k = tt - yl * hL, y = x.y0 + yl;
+      const int par = (1 + y) & 1, xx = 2 * k + par;
+      int kw, ke;
+      x_neighbours(k, par, hL, kw, ke);
+      const int ys = (y == L - 1) ? 0 : y + 1;
+      const int sk = slot ^ swz(x, k);
+      const word_t s1 = x.sm[lrow(x, 1, 0, yl) + k * ns + sk];
+      const word_t sw = x.sm[lrow(x, 0, 0, yl) + kw * ns + (slot ^ swz(x, kw))];
+      const word_t se = x.sm[lrow(x, 0, 0, yl) + ke * ns + (slot ^ swz(x, ke))];
+      const NbRow<CL> pn = north_row<CL>(x, 0, 0, yl), ps = south_row<CL>(x, 0, 0, yl);
+      const word_t sn = pn.template ld<1>(k * ns + sk).w[0];
+      const word_t ss = ps.template ld<1>(k * ns + sk).w[0];
+      const word_t okm = ok ? ~0ULL : 0ULL;
+      // couplings: west bond stored at the site (Jx of colour 1), east bond
+      // at the east neighbour (Jx of colour 0), north bond at the site (Jy
+      // of colour 1), south bond at the south neighbour (Jy of colour 0)
+      const word_t bw = (OPEN_X && xx == 0) ? 0 : (__ldg(J + 1 * x.half + y * hL + k) ^ s1 ^ sw) & okm;
+      const word_t be = (OPEN_X && xx == L - 1) ? 0 : (__ldg(J + 0 * x.half + y * hL + ke) ^ s1 ^ se) & okm;
+      const word_t bn = (__ldg(J + 3 * x.half + y * hL + k) ^ s1 ^ sn) & okm;
+      const word_t bs = (__ldg(J + 2 * x.half + ys * hL + k) ^ s1 ^ ss) & okm;
+      word_t c0, c1, c2;
+      count4(bw, be, bn, bs, c0, c1, c2);
+      add3_w<W0>(big, c0, c1, c2);
+      if (++held == 7) {
+        flush_pair_counts<W0>(big, cnt);
+        held = 0;
+      }
+    }
+  }
+  if (held) flush_pair_counts<W0>(big, cnt);
 }
 
 }  // namespace sa
