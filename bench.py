@@ -85,11 +85,25 @@ def c4_instances(n: int, index_offset: int = 0):
     return [(SHAPES[p][0], SHAPES[p][1], 1000 + index_offset + k) for k, p in enumerate(picks)]
 
 
-def shard_instances(rank: int, world: int, n: int):
+def shard_instances(rank: int, world: int, n: int, shape=None):
     """Rank `rank`'s share of a `world`-rank run: instances [rank*n, (rank+1)*n)
-    of the global sequence (weak scaling: n per rank, no overlap)."""
+    of the global sequence (weak scaling: n per rank, no overlap). With
+    `shape` = (lattice, L) every instance has that one shape (a small case of
+    one group of the mix, for profiling)."""
     assert 0 <= rank < world
+    if shape is not None:
+        return [(shape[0], shape[1], 1000 + rank * n + k) for k in range(n)]
     return c4_instances(n, index_offset=rank * n)
+
+
+def parse_shape(text):
+    """'LAT:L' (lattice 0 = 2D, 2 = 3D) -> (lattice, L), or None."""
+    if not text:
+        return None
+    lat, L = (int(v) for v in text.split(":"))
+    if (lat, L) not in SHAPES:
+        raise SystemExit(f"--shape {text}: not a shape of the mix {SHAPES}")
+    return lat, L
 
 
 def max_over_ranks(values, dist, device):
@@ -365,10 +379,16 @@ def serving_run(n: int, rate: float, budget_gb: float, chunk: int = 100):
 # ----------------------------------------------------------------------------- GPU
 def c4_config(args, world: int) -> dict:
     S = args.sweeps_per_step
-    return {"workload": f"batched PT mix: {args.instances} instances x 16 slots, 2D L{{16..64}} / "
-                        f"3D L{{8..24}}, {S} sweeps + exchange per sweep per step",
+    shape = parse_shape(getattr(args, "shape", None))
+    if shape is not None:
+        kind = "3D" if shape[0] == 2 else "2D"
+        what = f"one group of the mix: {args.instances} instances of {kind} L={shape[1]} x 16 slots"
+    else:
+        what = f"batched PT mix: {args.instances} instances x 16 slots, 2D L{{16..64}} / 3D L{{8..24}}"
+    return {"workload": f"{what}, {S} sweeps + exchange per sweep per step",
             "instances_per_gpu": args.instances, "slots": 16, "sweeps_per_step": S,
-            "l2": "inputs larger than L2 (1.9 GB of spins)",
+            "l2": ("inputs larger than L2 (1.9 GB of spins)" if shape is None
+                   else "one-shape case: spins of all its instances, see instances"),
             "parallelism": f"instances sharded, {world} GPU(s), no collective"}
 
 
@@ -438,7 +458,7 @@ def run_ours(args):
     world, rank, local, dist = init_ranks("nccl")
     torch.cuda.set_device(local)
 
-    insts = shard_instances(rank, world, args.instances)
+    insts = shard_instances(rank, world, args.instances, parse_shape(args.shape))
     stream = torch.cuda.Stream()
     b = build_c4_batch(insts, stream.cuda_stream, group_timing=True)
     S = args.sweeps_per_step
@@ -666,6 +686,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--sweeps-per-step", type=int, default=100)
     ap.add_argument("--instances", type=int, default=4096)
+    ap.add_argument("--shape", default=None, metavar="LAT:L",
+                    help="every instance of this one shape of the mix (e.g. 2:24; a small case for profiling)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-step-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
