@@ -634,7 +634,16 @@ __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, CL, SEG, HR>(), re
       // counts are already there (own): the barrier after the colour-1 half
       // made them complete.
       if (!own) {
-        rmeasure<CL, 4>(x, d3, open, a, nsl, s_cnt, hist_now);
+        if (d3 && xchg) {
+          // one counter of the pair's difference (rmeasure_pair_3d)
+          if (hist_now) {
+            for (int t = threadIdx.x; t < 128; t += blockDim.x) (&s_cnt[0][0])[t] = 0;
+            __syncthreads();
+          }
+          rmeasure_pair_3d<CL>(x, a, s_cnt);
+        } else {
+          rmeasure<CL, 4>(x, d3, open, a, nsl, s_cnt, hist_now);
+        }
         sync_all();
       }
       if (xchg) {
@@ -647,13 +656,17 @@ __global__ void __launch_bounds__(res_max_threads<P, SL, LAT, CL, SEG, HR>(), re
             for (int r = 0; r < C; ++r) {
               const unsigned* rc = cluster.map_shared_rank(&s_cnt[0][0], (unsigned)r);
               v0 += rc[j];
-              v1 += rc[64 + j];
+              if (!(d3 || own)) v1 += rc[64 + j];
             }
           } else {
             v0 = s_cnt[0][j];
             v1 = s_cnt[1][j];
           }
-          const int64_t dE = 2 * ((int64_t)v1 - (int64_t)v0);
+          // v0 = the difference counter D of the pair (3D, and 2D counted per
+          // warp): v(a+1) - v(a) = D - nbonds; else v0, v1 = the two slots'
+          // satisfied-bond counts (2D sweeps with a histogram pass)
+          const int64_t dv = (d3 || own) ? (int64_t)v0 - (int64_t)d.nbonds : (int64_t)v1 - (int64_t)v0;
+          const int64_t dE = 2 * dv;
           const bool acc = dE >= dc.lo && dE <= dc.hi;
           const unsigned bal = __ballot_sync(0xffffffffu, acc);
           if (lane == 0) s_mask[threadIdx.x >> 5] = bal;

@@ -961,89 +961,165 @@ __device__ __forceinline__ void rmeasure(const ResCtx& x, bool d3, bool open, in
 }
 
 // ---------------------------------------------------------------------------
-// The exchange pair's satisfied-bond counts in 2D, taken by each warp over its
-// own sites right after its colour-1 walk, with no barrier and no separate
-// pass. Every 2D bond joins a colour-0 and a colour-1 site, so the colour-1
-// sites' four bonds (west and east across an open x edge excepted) cover the
-// lattice once. They are final when this warp has walked its colour-1 tiles:
-// colour 0 was final at the barrier before the colour-1 half, and only this
-// warp writes the colour-1 sites of its tiles (rhalf_2d's tiles: 32 sites
-// from 32 * warp, stepping 32 * warps). Lanes: 16 sites x slots a, a+1; the
-// counts go into cnt[slot - a][replica], as rmeasure's do. (In 3D the same
-// scheme needs the z-bonds of both colours and measured slower than the
-// separate pass.)
+// The 3D exchange pass. The decision needs only E(a+1) - E(a) per replica, so
+// one counter takes, for every bond, b(a+1) + (1 - b(a)) (b = J ^ s_i ^ s_j,
+// the bits rmeasure counts): its total D gives v(a+1) - v(a) = D - nbonds.
+// One lane holds both slots of a site, so a site's three coupling words
+// (west, north, z-1: each site counts the bonds stored at it) are loaded once
+// for both, and a warp sums one counter instead of two. Lane t takes column
+// task t % T of T = 2 * columns (consecutive lanes, consecutive columns: the
+// slot swizzle spreads their words over the banks) and planes t / T, t / T +
+// phases, ...; a CTA with fewer threads than tasks loops over them. D goes
+// into cnt[0][replica].
 // ---------------------------------------------------------------------------
 template <int W0>
-__device__ __forceinline__ void add3_w(VCount<16>& big, word_t c0, word_t c1, word_t c2) {
+__device__ __forceinline__ void add3_plane(VCount<16>& big, word_t c0, word_t c1, word_t c2) {
   word_t carry = 0;
 #pragma unroll
   for (int b = 0; b < W0; ++b) {
     const word_t q = (b == 0) ? c0 : (b == 1) ? c1 : (b == 2) ? c2 : 0;
-    const word_t a = big.p[b];
-    big.p[b] = a ^ q ^ carry;
-    carry = (a & q) | (carry & (a ^ q));
+    const word_t v = big.p[b];
+    big.p[b] = v ^ q ^ carry;
+    carry = (v & q) | (carry & (v ^ q));
   }
 }
 
-template <int W0>
-__device__ __forceinline__ void flush_pair_counts(VCount<16>& big, unsigned (*cnt)[64]) {
-  const int lane = threadIdx.x & 31;
-  warp_sum_grow<2, W0>(big);
-  constexpr int NBU = W0 + 4;
-#pragma unroll
-  for (int m = 0; m < 4; ++m) {
-    const int j = (lane >> 1) + 16 * m;
-    atomicAdd(&cnt[lane & 1][j], big.template count_low<NBU>(j));
-  }
+template <bool CL>
+__device__ __forceinline__ void rmeasure_pair_3d(const ResCtx& x, int a, unsigned (*cnt)[64]) {
+  constexpr int W0 = 5;  // a lane adds at most 6 per site: a warp sum every 5 sites
+  const int lane = threadIdx.x & 31, t = threadIdx.x, nthr = blockDim.x;
+  const int L = x.L, hL = x.hL, ns = x.ns, cols = x.ny * hL;
+  const int T = 2 * cols;
+  const int phases = max(1, nthr / T);
+  const int rounds = (T + nthr - 1) / nthr;  // > 1 only when nthr < T
+  const int iters = (L + phases - 1) / phases;
+  const int zs = x.ny * x.rowW, zg = L * hL;
+  const long hf = x.half;
+  VCount<16> big;
   big.clear();
+  int held = 0;  // sites added since the last warp sum (warp-uniform)
+  auto flush = [&]() {
+    warp_sum_grow<1, W0>(big);
+    constexpr int NBU = W0 + 5;
+    atomicAdd(&cnt[0][lane], big.template count_low<NBU>(lane));
+    atomicAdd(&cnt[0][lane + 32], big.template count_low<NBU>(lane + 32));
+    big.clear();
+  };
+  const int zi = (nthr >= T) ? t / T : 0;
+  for (int r = 0; r < rounds; ++r) {
+    const int task = (nthr >= T) ? t % T : t + r * nthr;
+    const bool tok = (nthr >= T) ? t < phases * T : task < T;
+    const int tk = tok ? task : 0;  // idle lanes read column 0 and count nothing
+    const int c = tk >= cols ? 1 : 0, oc = 1 - c;
+    const int col = tk - c * cols;
+    const int yl = div_hl(col, x);
+    const int k = col - yl * hL, y = x.y0 + yl;
+    int kw, ke;
+    x_neighbours(k, (c + y) & 1, hL, kw, ke);
+    const int sa = a ^ swz(x, k), sb = (a + 1) ^ swz(x, k);
+    const int wa = a ^ swz(x, kw), wb = (a + 1) ^ swz(x, kw);
+    const int own = lrow(x, c, 0, yl) + k * ns;
+    const int wrow = lrow(x, oc, 0, yl) + kw * ns;
+    NbRow<CL> pn = north_row<CL>(x, oc, 0, yl);
+    pn.step(k * ns);
+    const int zsn = (yl > 0) ? zs : x.nyN * x.rowW;
+    const word_t* Jc = x.J + (long)c * hf + (y * hL + k);
+#pragma unroll 1
+    for (int it = 0; it < iters; ++it) {  // warp-uniform
+      const int z = zi + it * phases;
+      const bool ok = tok && z < L;
+      const int zz = ok ? z : 0, zu = (zz == 0) ? L - 1 : zz - 1;
+      const word_t* jp = Jc + zz * zg;
+      const word_t jw = __ldg(jp), jn = __ldg(jp + 2 * hf), ju = __ldg(jp + 4 * hf);
+      const int o = own + zz * zs, ou = own + zu * zs, ow = wrow + zz * zs;
+      const word_t ai = x.sm[o + sa], bi = x.sm[o + sb];
+      const word_t aw = x.sm[ow + wa], bw = x.sm[ow + wb];
+      const word_t an = pn.template ld<1>(zz * zsn + sa).w[0], bn = pn.template ld<1>(zz * zsn + sb).w[0];
+      const word_t au = x.sm[ou + sa], bu = x.sm[ou + sb];
+      const word_t okm = ok ? ~0ULL : 0ULL;
+      word_t c0, c1, c2;
+      count6((jw ^ bi ^ bw) & okm, (jn ^ bi ^ bn) & okm, (ju ^ bi ^ bu) & okm,
+             ~(jw ^ ai ^ aw) & okm, ~(jn ^ ai ^ an) & okm, ~(ju ^ ai ^ au) & okm, c0, c1, c2);
+      add3_plane<W0>(big, c0, c1, c2);
+      if (++held == 5) {
+        flush();
+        held = 0;
+      }
+    }
+  }
+  if (held) flush();
 }
 
+// ---------------------------------------------------------------------------
+// The 2D exchange counts, taken by each warp over its own sites right after
+// its colour-1 walk, with no barrier and no separate pass; the same difference
+// counter D as rmeasure_pair_3d, into cnt[0][replica]. Every 2D bond joins a
+// colour-0 and a colour-1 site, so the colour-1 sites' four bonds (west and
+// east across an open x edge excepted) cover the lattice once. They are final
+// when this warp has walked its colour-1 tiles: colour 0 was final at the
+// barrier before the colour-1 half, and only this warp writes the colour-1
+// sites of its tiles (rhalf_2d's tiles: 32 sites from 32 * warp, stepping
+// 32 * warps). Lane = site of the tile, both slots. (In 3D the same scheme
+// needs the z-bonds of both colours and measured slower than a separate pass.)
+// ---------------------------------------------------------------------------
 template <bool OPEN_X, bool CL>
 __device__ __forceinline__ void rmeasure_own_2d(const ResCtx& x, int a, unsigned (*cnt)[64]) {
-  constexpr int W0 = 5;  // a lane adds at most 4 per site: a warp sum every 7 sites
+  constexpr int W0 = 5;  // a lane adds at most 8 per site: a warp sum every 3 sites
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int g = lane >> 1, slot = a + (lane & 1);
   const int L = x.L, hL = x.hL, ns = x.ns, tot = x.ny * hL;
   const word_t* J = x.J;
   VCount<16> big;
   big.clear();
   int held = 0;  // sites added since the last warp sum (warp-uniform)
+  auto flush = [&]() {
+    warp_sum_grow<1, W0>(big);
+    constexpr int NBU = W0 + 5;
+    atomicAdd(&cnt[0][lane], big.template count_low<NBU>(lane));
+    atomicAdd(&cnt[0][lane + 32], big.template count_low<NBU>(lane + 32));
+    big.clear();
+  };
   for (int base = warp * 32; base < tot; base += nwarps * 32) {
-    for (int h = 0; h < 32; h += 16) {
-      const int t = base + h + g;
-      const bool ok = t < tot;
-      const int tt = ok ? t : base;  // lanes past the end read a real site and count nothing
-      const int yl = div_hl(tt, x);
-      const int k = tt - yl * hL, y = x.y0 + yl;
-      const int par = (1 + y) & 1, xx = 2 * k + par;
-      int kw, ke;
-      x_neighbours(k, par, hL, kw, ke);
-      const int ys = (y == L - 1) ? 0 : y + 1;
-      const int sk = slot ^ swz(x, k);
-      const word_t s1 = x.sm[lrow(x, 1, 0, yl) + k * ns + sk];
-      const word_t sw = x.sm[lrow(x, 0, 0, yl) + kw * ns + (slot ^ swz(x, kw))];
-      const word_t se = x.sm[lrow(x, 0, 0, yl) + ke * ns + (slot ^ swz(x, ke))];
-      const NbRow<CL> pn = north_row<CL>(x, 0, 0, yl), ps = south_row<CL>(x, 0, 0, yl);
-      const word_t sn = pn.template ld<1>(k * ns + sk).w[0];
-      const word_t ss = ps.template ld<1>(k * ns + sk).w[0];
-      const word_t okm = ok ? ~0ULL : 0ULL;
-      // couplings: west bond stored at the site (Jx of colour 1), east bond
-      // at the east neighbour (Jx of colour 0), north bond at the site (Jy
-      // of colour 1), south bond at the south neighbour (Jy of colour 0)
-      const word_t bw = (OPEN_X && xx == 0) ? 0 : (__ldg(J + 1 * x.half + y * hL + k) ^ s1 ^ sw) & okm;
-      const word_t be = (OPEN_X && xx == L - 1) ? 0 : (__ldg(J + 0 * x.half + y * hL + ke) ^ s1 ^ se) & okm;
-      const word_t bn = (__ldg(J + 3 * x.half + y * hL + k) ^ s1 ^ sn) & okm;
-      const word_t bs = (__ldg(J + 2 * x.half + ys * hL + k) ^ s1 ^ ss) & okm;
-      word_t c0, c1, c2;
-      count4(bw, be, bn, bs, c0, c1, c2);
-      add3_w<W0>(big, c0, c1, c2);
-      if (++held == 7) {
-        flush_pair_counts<W0>(big, cnt);
-        held = 0;
-      }
+    const int t = base + lane;
+    const bool ok = t < tot;
+    const int tt = ok ? t : base;  // lanes past the end read a real site and count nothing
+    const int yl = div_hl(tt, x);
+    const int k = tt - yl * hL, y = x.y0 + yl;
+    const int par = (1 + y) & 1, xx = 2 * k + par;
+    int kw, ke;
+    x_neighbours(k, par, hL, kw, ke);
+    const int ys = (y == L - 1) ? 0 : y + 1;
+    const int sa = a ^ swz(x, k), sb = (a + 1) ^ swz(x, k);
+    const int o1 = lrow(x, 1, 0, yl) + k * ns;
+    const int ow = lrow(x, 0, 0, yl) + kw * ns, oe = lrow(x, 0, 0, yl) + ke * ns;
+    const int wa = a ^ swz(x, kw), wb = (a + 1) ^ swz(x, kw);
+    const int ea = a ^ swz(x, ke), eb = (a + 1) ^ swz(x, ke);
+    NbRow<CL> pn = north_row<CL>(x, 0, 0, yl), ps = south_row<CL>(x, 0, 0, yl);
+    pn.step(k * ns);
+    ps.step(k * ns);
+    const word_t ai = x.sm[o1 + sa], bi = x.sm[o1 + sb];
+    const word_t aw = x.sm[ow + wa], bw = x.sm[ow + wb];
+    const word_t ae = x.sm[oe + ea], be = x.sm[oe + eb];
+    const word_t an = pn.template ld<1>(sa).w[0], bn = pn.template ld<1>(sb).w[0];
+    const word_t as = ps.template ld<1>(sa).w[0], bs = ps.template ld<1>(sb).w[0];
+    // couplings: west bond stored at the site (Jx of colour 1), east bond at
+    // the east neighbour (Jx of colour 0), north bond at the site (Jy of
+    // colour 1), south bond at the south neighbour (Jy of colour 0)
+    const word_t jw = __ldg(J + 1 * x.half + y * hL + k), je = __ldg(J + 0 * x.half + y * hL + ke);
+    const word_t jn = __ldg(J + 3 * x.half + y * hL + k), js = __ldg(J + 2 * x.half + ys * hL + k);
+    const word_t okm = ok ? ~0ULL : 0ULL;
+    const word_t mw = (OPEN_X && xx == 0) ? 0 : okm, me = (OPEN_X && xx == L - 1) ? 0 : okm;
+    // b(a+1) and 1 - b(a) for each existing bond
+    word_t p0, p1, p2, q0, q1, q2;
+    count4((jw ^ bi ^ bw) & mw, (je ^ bi ^ be) & me, (jn ^ bi ^ bn) & okm, (js ^ bi ^ bs) & okm, p0, p1, p2);
+    count4(~(jw ^ ai ^ aw) & mw, ~(je ^ ai ^ ae) & me, ~(jn ^ ai ^ an) & okm, ~(js ^ ai ^ as) & okm, q0, q1, q2);
+    add3_plane<W0>(big, p0, p1, p2);
+    add3_plane<W0>(big, q0, q1, q2);
+    if (++held == 3) {
+      flush();
+      held = 0;
     }
   }
-  if (held) flush_pair_counts<W0>(big, cnt);
+  if (held) flush();
 }
 
 }  // namespace sa
