@@ -136,3 +136,37 @@ def test_explicit_shapes_and_fallback(sab):
     b.sync()
     check_instance(b, 0, O.LAT_3D, 10, T5, 5, 6, 7)
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("lat,L,nslots,shape", [
+    # 3D on one CTA of two warps: 144 column tasks for 64 threads, so the
+    # exchange pass's lanes loop over tasks and walk every plane themselves
+    (O.LAT_3D, 12, 16, (1, 1, 2, 0)),
+    (O.LAT_3D, 12, 6, (1, 1, 2, 0)),
+    # 2D on small blocks: each warp walks and counts many tiles, with a warp
+    # sum every three sites
+    (O.LAT_2D, 32, 16, (1, 2, 2, 0)),
+    (O.LAT_2D_OPEN_X, 24, 10, (1, 2, 2, 0)),
+])
+def test_exchange_counts_in_narrow_blocks(sab, lat, L, nslots, shape):
+    """The exchange's difference counter in blocks with far fewer threads
+    than the lattice has columns (or sites per colour): decisions, masks and
+    spins still match parallel_tempering<>."""
+    from simulated_annealing_b200.batch import Batch
+    from test_gpu_batch import check_instance
+
+    T = list(np.geomspace(0.5, 2.0, nslots) if lat == O.LAT_3D else np.geomspace(0.3, 1.6, nslots))
+    b = Batch()
+    lad = b.add_ladder(T)
+    b.add_instance(lat, L, ladder=lad, seed_J=31 + L, seed=32 + L)
+    b.set_tuning([[lat, L, nslots, *shape]])
+    b.set_spread(False)
+    b.finalize()
+    assert b.shape(0) == (lat, L, nslots, *shape)
+    b.record_exchanges(16)
+    b.run(5)
+    b.run(4)
+    b.sync()
+    check_instance(b, 0, lat, L, T, 31 + L, 32 + L, 9)
+    b.close()
